@@ -1,0 +1,410 @@
+#!/usr/bin/env python3
+"""Benchmark of the force-and-step path on B200.
+
+Workload (one GPU): the Barnes-Hut warp walk on 1,000,000 particles (two
+exponential disks, seeded), theta 0.5, eps 0.05, dt 0.005, 30-bit Morton
+keys, tree rebuilt every step.  A step is one full leapfrog step: opening kick
++ drift + bounding box, Morton keys, onesweep radix sort, Karras build,
+centres of mass, warp walk with the closing kick fused.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0.  `value` = steps/s over the K timed steps (sum of
+per-step CUDA-event windows on the simulation's stream, L2 flushed by a
+256 MB write before every step, max over ranks; N ranks run N independent
+replicas).  `e2e` = the same metric through the C ABI with the state
+(pos, vel, a(x)) uploaded from pinned host memory before and downloaded after
+every step.  `roofline` = the warp walk, useful work 20 flop x per-thread-
+criterion interactions, against the FP32 FMA peak measured on this GPU by a
+calibration kernel.  `cpu_baseline` = the CPU oracle port (C + OpenMP) of the
+same step on this host's cores, on a sample of targets.
+
+--impl reference times that CPU port alone as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = ("steps/s at 1M (BH θ=0.5); served particle-steps/s + p99 vs "
+          "plain, equal error")
+N_DEFAULT = 1_000_000
+FLOP_PER_PAIR = 20          # src/main.cu:203-207 convention
+BUILD_BYTES_PER_PARTICLE = 230   # algorithmic HBM bytes of the tree build
+L2_FLUSH_BYTES = 256 << 20
+BH_KERNELS_PER_STEP = 9     # prep, morton, 4 sort passes, karras, com, walk
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--traverse", choices=["thread", "warp"], default="warp")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    return {"workload": "Barnes-Hut %s walk, N=%d, theta %.2g, eps 0.05, dt 0.005, "
+                        "30-bit Morton keys, tree rebuilt every step" %
+                        (args.traverse, args.n, args.theta),
+            "n": args.n, "theta": args.theta, "traverse": args.traverse,
+            "key_bits": 30, "dt": 0.005, "eps": 0.05,
+            "l2": "flushed before every timed step (256 MB write)",
+            "parallelism": "replicas (one independent simulation per GPU)"}
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing
+# --------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def dist_max(pg, value):
+    if pg is None:
+        return value
+    import torch
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# --------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="nb_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return float("nan")
+        sm = [num(r[1]) for r in rows]
+        mx = max(num(r[2]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for r in rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "samples": len(rows), "reasons": sorted(reasons),
+                "power_w_max": max(num(r[3]) for r in rows)}
+
+
+# --------------------------------------------------------------------------
+# CPU port (the oracle), used for cpu_baseline and the reference arm
+# --------------------------------------------------------------------------
+def cpu_step_sample(pos, vel, theta, traverse, sample, rng):
+    """One leapfrog step of the CPU port on all particles (kick, drift, LBVH
+    build) with the tree walk on `sample` random targets; returns the
+    extrapolated seconds for the full step."""
+    from oracle import oracle as O
+    n = pos.shape[0]
+    acc0 = np.zeros_like(pos)
+    t0 = time.perf_counter()
+    vh = O.kick(vel, acc0, 0.0025)
+    p1, _ = O.drift(pos, None, vh, 0.005, True)
+    tree = O.Tree(p1, 30)
+    t1 = time.perf_counter()
+    if traverse == "warp":
+        nw = (n + 31) // 32
+        w = np.sort(rng.choice(nw, max(1, sample // 32), replace=False))
+        tree.walk_warp(theta, 0.05, 1.0, w)
+        frac = nw / w.shape[0]
+    else:
+        tg = np.sort(rng.choice(n, sample, replace=False))
+        tree.walk_thread(theta, 0.05, 1.0, tg)
+        frac = n / sample
+    t2 = time.perf_counter()
+    return (t1 - t0) + (t2 - t1) * frac, (t1 - t0), (t2 - t1)
+
+
+def cpu_baseline(args, steps=2):
+    from nbodyssey_b200 import ic
+    from oracle import oracle as O
+    pos, vel = ic.bh_config(args.n, seed=0)
+    rng = np.random.default_rng(0)
+    times = []
+    for _ in range(steps):
+        t, tb, tw = cpu_step_sample(pos, vel, args.theta, args.traverse,
+                                    args.cpu_sample, rng)
+        times.append(t)
+    best = min(times)
+    return {"value": 1.0 / best, "unit": "steps/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": ("CPU oracle (C, OpenMP): kick + compensated drift + full LBVH "
+                       "build of all %d particles, %s walk of %d sampled targets, "
+                       "walk time scaled by N/sample; best of %d steps" %
+                       (args.n, args.traverse, args.cpu_sample, steps))}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    cb = cpu_baseline(args, steps=steps)
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s",
+            "n_gpus": world, "steps": steps, "warmup": 0,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload(args), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# B200 arm
+# --------------------------------------------------------------------------
+def pinned_array(lib, shape, keep):
+    from nbodyssey_b200 import _lib as L
+    nbytes = int(np.prod(shape)) * 4
+    p = ctypes.c_void_p()
+    L.check(lib.nb_alloc_pinned(nbytes, ctypes.byref(p)))
+    keep.append(p)
+    buf = (ctypes.c_float * int(np.prod(shape))).from_address(p.value)
+    return np.ctypeslib.as_array(buf).reshape(shape)
+
+
+def interactions(sim, api, params):
+    """Sum over particles of the per-thread-criterion interaction count."""
+    from dataclasses import replace
+    sim.set_params(replace(params, traverse="thread"))
+    _, cnt = sim.debug_forces()
+    sim.set_params(params)
+    return int(cnt.astype(np.int64).sum())
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return {}
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the walk kernel from the committed ncu
+    summary (profiles/), if present."""
+    path = os.path.join(ROOT, "profiles", "walk_warp_1m.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def run_b200(args, rank, world, local, pg):
+    from nbodyssey_b200 import _lib as L
+    from nbodyssey_b200 import api, ic
+    lib = L.load()
+    L.check(lib.nb_set_device(local))
+    params = api.SimParams(dt=0.005, epsilon=0.05, theta=args.theta, force="bh",
+                           traverse=args.traverse, key_bits=30, compensated=True)
+    pos, vel = ic.bh_config(args.n, seed=rank)
+    sim = api.Simulation(pos, vel, params)
+    n = args.n
+
+    # FP32 peak of this GPU (calibration kernel), before the sim's work
+    ps, pp = ctypes.c_double(), ctypes.c_double()
+    L.check(lib.nb_measure_fp32_peak(ctypes.byref(ps), ctypes.byref(pp)))
+    fp32_peak = max(ps.value, pp.value)
+
+    inter0 = interactions(sim, api, params)
+
+    # warm-up (graph path), then timed steps with per-phase events
+    sim.step(args.warmup)
+    sim.sync()
+    sim.reset_timing()
+    sim.set_timing(True)
+    clocks = Clocks(local)
+    dist_barrier(pg)
+    clocks.start()
+    for _ in range(args.steps):
+        L.check(lib.nb_flush_l2(sim._h, L2_FLUSH_BYTES))
+        sim.step(1)
+    sim.sync()
+    clk = clocks.stop()
+    phases, calls = sim.phase_times()
+    total_ms, fcalls = sim.force_timing()
+    sim.set_timing(False)
+    assert calls == args.steps and fcalls == args.steps, (calls, fcalls)
+    dist_barrier(pg)
+    total_ms = dist_max(pg, total_ms)
+    inter1 = interactions(sim, api, params)
+    inter = 0.5 * (inter0 + inter1)
+
+    # steady state through the captured graph, no flush (informational)
+    sim.record(0)
+    sim.step(args.steps)
+    sim.record(1)
+    graph_ms = sim.elapsed_ms(0, 1)
+
+    # end to end: pinned host state in, step, state out, every step
+    keep = []
+    hp = pinned_array(lib, (n, 4), keep)
+    hv = pinned_array(lib, (n, 4), keep)
+    ha = pinned_array(lib, (n, 4), keep)
+    L.check(lib.nb_get_positions(sim._h, L.ptr(hp)))
+    L.check(lib.nb_get_velocities(sim._h, L.ptr(hv)))
+    L.check(lib.nb_get_accelerations(sim._h, L.ptr(ha)))
+    for it in range(args.e2e_steps + 2):
+        if it == 2:
+            dist_barrier(pg)
+            t0 = time.perf_counter()
+        L.check(lib.nb_set_state_acc(sim._h, L.ptr(hp), L.ptr(hv), L.ptr(ha)))
+        L.check(lib.nb_step(sim._h, 1))
+        L.check(lib.nb_get_positions(sim._h, L.ptr(hp)))
+        L.check(lib.nb_get_velocities(sim._h, L.ptr(hv)))
+        L.check(lib.nb_get_accelerations(sim._h, L.ptr(ha)))
+    e2e_s = dist_max(pg, time.perf_counter() - t0)
+    for p in keep:
+        lib.nb_free_pinned(p)
+    sim.close()
+
+    if rank != 0:
+        return
+    steps_total = args.steps * world
+    value = steps_total / (total_ms * 1e-3)
+    walk_ms = phases["walk"] / calls
+    achieved = FLOP_PER_PAIR * inter / (walk_ms * 1e-3) / 1e12
+    build_ms = sum(phases[k] for k in ("prep", "morton", "sort", "build", "com")) / calls
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    traffic = profiled_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded two exponential disks (R_d 1 cut at 5, "
+                "sigma_z 0.1, 0.05 v_c dispersion, centres (-+10,-+2,0), "
+                "bulk -+0.25, B tilted 30 deg)",
+        "config": workload(args),
+        "particle_steps_per_s": value * n,
+        "graph_steps_per_s_no_flush": world * args.steps / (graph_ms * 1e-3),
+        "phases_ms_per_step": {k: v / calls for k, v in phases.items() if v > 0},
+        "interactions_per_particle": inter / n,
+        "gpu_launches": BH_KERNELS_PER_STEP * args.steps,
+        "e2e": {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
+                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
+                "path": "nb_set_state_acc + nb_step + nb_get_{positions,"
+                        "velocities,accelerations}, pinned host buffers, wall clock"},
+        "roofline": {"kernel": "k_walk_%s" % args.traverse, "bound": "fp32",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": traffic,
+                     "work": "20 flop x per-thread-criterion interactions "
+                             "(%.4g per step)" % inter,
+                     "peak_source": "measured on this GPU: FP32 FMA calibration "
+                                    "kernel (scalar %.1f, packed f32x2 %.1f TFLOP/s)" %
+                                    (ps.value, pp.value)},
+        "roofline_build": {"bound": "hbm", "achieved":
+                           BUILD_BYTES_PER_PARTICLE * n / (build_ms * 1e-3) / 1e9,
+                           "peak": hbm, "unit": "GB/s",
+                           "frac": (BUILD_BYTES_PER_PARTICLE * n / (build_ms * 1e-3) / 1e9
+                                    / hbm) if hbm else None,
+                           "work": "230 B/particle (bbox, keys, 4 sort passes, "
+                                   "gather, build, centres of mass)",
+                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_b200(args, rank, world, local, pg)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+/*
+ * nbody_b200.h -- C ABI of the B200-native nbodyssey force-and-step path.
+ *
+ * Plain C types only (pointers, sizes, POD structs).  Every function returns
+ * an int status (NB_OK on success); nb_last_error() gives a thread-local
+ * message for the last failure on the calling thread.  Host arrays passed in
+ * are owned by the caller and copied; device state behind a handle is owned
+ * by the library.  A handle may be used by one host thread at a time.
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the nbodyssey project).  The reference aborts the process on any CUDA error
+ * (src/cuda_check.cuh:7-15) and on bad input (src/main.cu:28-31, 118-126);
+ * here the same conditions return a status instead.
+ */
+#ifndef NBODY_B200_H
+#define NBODY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define NB_API __attribute__((visibility("default")))
+#else
+#define NB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NB_OK 0
+#define NB_ERR_INVALID 1 /* bad argument: n, eps <= 0, theta < 0, key_bits, NULL */
+#define NB_ERR_CUDA 2    /* a CUDA runtime call failed (message has the call) */
+#define NB_ERR_DEVICE 3  /* a kernel raised its error word (see NB_DEVERR_*) */
+#define NB_ERR_NOMEM 4   /* device allocation failed, or over the HBM budget */
+#define NB_ERR_IO 5      /* file open / read / write failed, truncated file */
+#define NB_ERR_STATE 6   /* call not valid in the object's current state */
+#define NB_ERR_NOTFOUND 7 /* unknown request / simulation id */
+
+/* bits of the device error word (NB_ERR_DEVICE) */
+#define NB_DEVERR_STACK 1u  /* a tree walk's stack would have overflowed */
+#define NB_DEVERR_SORT 2u   /* a radix-sort look-back wait hit its limit */
+#define NB_DEVERR_WAIT 4u   /* a bulk-copy barrier wait hit its limit */
+#define NB_DEVERR_QUEUE 8u  /* a persistent work-queue wait hit its limit */
+
+/* ---- parameters (src/simulation.hpp:4-15: SimParams, ForceMethod,
+ *      BhTraversal) ------------------------------------------------------- */
+#define NB_FORCE_NAIVE 0      /* ForceMethod::kNaive, tiled all-pairs */
+#define NB_FORCE_BH 1         /* ForceMethod::kBarnesHut, LBVH rebuilt per step */
+#define NB_TRAVERSE_THREAD 0  /* BhTraversal::kThread, one walk per particle */
+#define NB_TRAVERSE_WARP 1    /* BhTraversal::kWarp, one shared walk per warp */
+
+typedef struct nb_params {
+  float dt;            /* timestep (reference default 0.01, src/main.cu:25) */
+  float eps;           /* Plummer softening length, > 0 (default 0.05) */
+  float G;             /* gravitational constant (default 1) */
+  float theta;         /* BH opening angle, >= 0; 0 = exact (default 0.5) */
+  int32_t force;       /* NB_FORCE_* (default naive) */
+  int32_t traverse;    /* NB_TRAVERSE_* (default thread) */
+  int32_t key_bits;    /* Morton key width: 30 (10 bits/axis, uint32 keys) or
+                          63 (21 bits/axis, the reference's width) */
+  int32_t compensated; /* 1: positions kept as a hi/lo float pair through the
+                          drift (forces use hi); 0: plain float drift */
+} nb_params;
+
+/* Fills the reference defaults: dt 0.01, eps 0.05, G 1, theta 0.5, naive,
+ * thread, 30-bit keys, compensated drift on. */
+NB_API void nb_params_default(nb_params* p);
+
+NB_API const char* nb_last_error(void);
+NB_API int nb_version(void);
+/* Number of CUDA devices visible (0 on a machine without a GPU). */
+NB_API int nb_device_count(int* out);
+/* Device used by this thread's later calls (one process per GPU). */
+NB_API int nb_set_device(int device);
+/* Page-locked host buffers, for asynchronous host<->device copies. */
+NB_API int nb_alloc_pinned(size_t bytes, void** out);
+NB_API int nb_free_pinned(void* p);
+/* Measures the FP32 FMA throughput of the current device with two
+ * calibration kernels (scalar fma.rn.f32 and packed fma.rn.f32x2 chains over
+ * all SMs); tflops = 2 * FMAs / time.  Used as the roofline denominator of
+ * the FP32-pipe-bound force kernels. */
+NB_API int nb_measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
+
+/* ======================================================================
+ * Handle API: one simulation whose state lives on the device.
+ * ==================================================================== */
+typedef struct nb_sim nb_sim;
+
+/* ParticleSystem::allocate + upload (src/simulation.cu:4-20).  pos4 = n rows
+ * of (x, y, z, m), vel4 = n rows of (vx, vy, vz, _), host memory. */
+NB_API int nb_sim_create(int n, const float* pos4, const float* vel4,
+                  const nb_params* p, nb_sim** out);
+/* ParticleSystem::release + bh_release (src/simulation.cu:10-15,
+ * src/forces_bh.cu:541-548). */
+NB_API int nb_sim_destroy(nb_sim* s);
+NB_API int nb_sim_n(const nb_sim* s, int* n);
+NB_API int nb_set_params(nb_sim* s, const nb_params* p);
+NB_API int nb_get_params(const nb_sim* s, nb_params* p);
+/* Replace the state from host arrays (upload, src/simulation.cu:17-20). */
+NB_API int nb_set_state(nb_sim* s, const float* pos4, const float* vel4);
+/* ParticleSystem::download_positions (src/simulation.cu:22-24): n float4,
+ * positions rounded to float (hi part), mass in w. */
+NB_API int nb_get_positions(nb_sim* s, float* pos4);
+NB_API int nb_get_velocities(nb_sim* s, float* vel4);
+/* Low-order position parts (compensated mode; zeros otherwise). */
+NB_API int nb_get_position_lo(nb_sim* s, float* lo4);
+/* The acceleration buffer a(x) (after a step it holds a(x_new)). */
+NB_API int nb_get_accelerations(nb_sim* s, float* acc4);
+/* Upload a state together with its a(x), so the next step needs no priming
+ * force evaluation (a host round trip of pos / vel / acc between steps). */
+NB_API int nb_set_state_acc(nb_sim* s, const float* pos4, const float* vel4,
+                            const float* acc4);
+
+/* compute_forces (src/forces.cuh:8, src/forces.cu:68-86): a(x) for the
+ * current positions into the simulation's acceleration buffer, in original
+ * particle order; copied to acc4 (host, n float4, w = 0) when non-NULL. */
+NB_API int nb_compute_forces(nb_sim* s, float* acc4);
+/* leapfrog_step x nsteps (src/integrator.cuh:19, src/integrator.cu:27-37):
+ * kick, drift, forces, kick.  The first call after create / set_state first
+ * computes a(x0) as src/main.cu:184 does.  Enqueued asynchronously on the
+ * simulation's stream; errors of the kernels surface at the next sync. */
+NB_API int nb_step(nb_sim* s, int nsteps);
+/* Waits for the simulation's stream and checks the device error word. */
+NB_API int nb_sync(nb_sim* s);
+/* total_energy (src/integrator.cuh:21, src/integrator.cu:93-110), FP64
+ * reductions: e3 = {E, KE, PE}; mom3 = total momentum (may be NULL). */
+NB_API int nb_energy(nb_sim* s, double* e3, double* mom3);
+
+/* Force timing (src/forces.cu:62-66, 88-90): CUDA-event time of every force
+ * evaluation, accumulated when timing is on (off by default). */
+NB_API int nb_set_timing(nb_sim* s, int enable);
+NB_API int nb_force_timing(nb_sim* s, double* ms_total, long* calls);
+NB_API int nb_reset_timing(nb_sim* s);
+/* Per-phase times (bh_report_phase_timing, src/forces_bh.cu:529-539):
+ * ms[NB_PHASES] accumulated over all timed steps, calls = steps timed. */
+#define NB_PHASES 8
+#define NB_PHASE_PREP 0     /* kick + drift + bounding box (+ source packing) */
+#define NB_PHASE_MORTON 1
+#define NB_PHASE_SORT 2
+#define NB_PHASE_BUILD 3
+#define NB_PHASE_COM 4
+#define NB_PHASE_WALK 5     /* traversal, or the all-pairs force kernel */
+#define NB_PHASE_ENERGY 6
+#define NB_PHASE_OTHER 7
+NB_API int nb_phase_times(nb_sim* s, double* ms, long* calls);
+
+/* Events on the simulation's stream, for callers that time whole regions. */
+NB_API int nb_record(nb_sim* s, int slot /* 0..15 */);
+NB_API int nb_elapsed_ms(nb_sim* s, int slot0, int slot1, double* ms);
+
+/* Use a captured CUDA graph for each step (default on).  The graph is
+ * re-captured when the parameters change. */
+NB_API int nb_set_graphs(nb_sim* s, int enable);
+/* Enqueues a write of `bytes` (>= the 126 MB L2) to a scratch buffer on the
+ * simulation's stream, evicting the state from L2 between timed steps. */
+NB_API int nb_flush_l2(nb_sim* s, size_t bytes);
+
+/* Debug / parity: run the tree build on the current positions and copy out
+ * keys (uint64 per particle, sorted), the permutation (sorted -> original),
+ * children [n-1][2], parent [2n-1], node com4 [n-1][4] and size2 [n-1].
+ * Any pointer may be NULL. */
+NB_API int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
+                  int32_t* children, int32_t* parent, float* com4,
+                  float* size2);
+/* Debug / parity: forces with per-particle interaction counts (original
+ * order; warp mode counts the warp's shared walk for every lane). */
+NB_API int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts);
+
+/* compare_forces (src/main.cu:75-112): naive vs Barnes-Hut on the current
+ * state, max and mean relative difference |a-b|/(|a|+1e-30). */
+NB_API int nb_compare_forces(nb_sim* s, double* max_rel, double* mean_rel);
+
+/* ======================================================================
+ * Device-pointer API: drop-ins for the reference's C++ functions, operating
+ * on caller-owned device arrays (float4 rows) on a caller-given stream
+ * (cudaStream_t passed as void*; NULL = legacy default stream).  Scratch is
+ * held by a workspace (the reference's process-global Scratch,
+ * src/forces_bh.cu:50-69), grown only when n grows.
+ * ==================================================================== */
+typedef struct nb_workspace nb_workspace;
+NB_API int nb_workspace_create(nb_workspace** out);
+NB_API int nb_workspace_destroy(nb_workspace* w); /* bh_release */
+
+/* compute_forces(sys, d_acc, p) (src/forces.cuh:8). */
+NB_API int nb_compute_forces_dev(nb_workspace* w, int n, const float* d_pos4,
+                          float* d_acc4, const nb_params* p, void* stream);
+/* leapfrog_step(sys, d_acc, p) (src/integrator.cuh:19): plain float drift
+ * (no low-order state); d_acc must hold a(x) on entry, a(x_new) on exit. */
+NB_API int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_vel4,
+                         float* d_acc4, const nb_params* p, void* stream);
+/* total_energy(sys, p) (src/integrator.cuh:21): synchronous, e3 on host. */
+NB_API int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,
+                        const float* d_vel4, const nb_params* p, double* e3,
+                        void* stream);
+
+/* ======================================================================
+ * Files and the run loop (src/main.cu:115-215, docs/FORMATS.md).
+ * ==================================================================== */
+/* load_ic (src/main.cu:115-128).  Call with pos4 = vel4 = NULL to get n. */
+NB_API int nb_read_ic(const char* path, int* n, float* pos4, float* vel4);
+NB_API int nb_write_ic(const char* path, int n, const float* pos4, const float* vel4);
+/* dump_frame (src/main.cu:130-138): <dir>/frame_%05d.bin. */
+NB_API int nb_write_frame(const char* dir, int index, int n, const float* pos4);
+/* One energy-log row, "%d,%.5f,%.8e,%.8e,%.8e,%.3e\n" with time = step*dt
+ * in float and rel = (E - E0)/|E0| (src/main.cu:172-178).  Host only. */
+NB_API int nb_format_energy_row(char* buf, size_t cap, int step, float dt, double e,
+                         double ke, double pe, double e0);
+
+typedef struct nb_run_stats {
+  double wall_s;        /* host wall time of the loop */
+  double force_ms;      /* CUDA-event time of the force evaluations */
+  long force_calls;
+  int frames;           /* frames written */
+  double e0, e_final, rel_final;
+  double phase_ms[NB_PHASES]; /* per-phase time per step (timing mode) */
+} nb_run_stats;
+/* The main loop of src/main.cu:140-215: E0, a(x0), then per step a
+ * leapfrog step; after every step with step % dump_every == 0 a frame
+ * (frame_%05d.bin, numbered from 0) and an energy row; a final row at
+ * `steps`.  Frames leave the device on a side stream into pinned buffers and
+ * are written by a host thread while the next steps run.  out_dir / csv may
+ * be NULL to skip frames / the log.  `timing` turns on the phase timers. */
+NB_API int nb_run(nb_sim* s, int steps, int dump_every, const char* out_dir,
+           const char* energy_csv, int timing, nb_run_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBODY_B200_H */

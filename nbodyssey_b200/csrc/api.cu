@@ -1,0 +1,868 @@
+// C ABI of the force-and-step path: workspace management, the simulation
+// handle, pipeline orchestration (eager or one captured CUDA graph per step),
+// phase timing, and the device-pointer drop-ins for compute_forces /
+// leapfrog_step / total_energy (src/forces.cuh:8, src/integrator.cuh:19-21).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "nb_internal.cuh"
+
+namespace nb {
+
+static thread_local std::string g_err;
+
+int set_error(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+const char* last_error() { return g_err.c_str(); }
+
+// ---------------------------------------------------------------------------
+// Workspace
+// ---------------------------------------------------------------------------
+template <typename T>
+static int dalloc(T** p, size_t count) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(NB_ERR_NOMEM, std::string("cudaMalloc of ") +
+                                       std::to_string(count * sizeof(T)) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+  }
+  return NB_OK;
+}
+
+static int ws_basic(Workspace& w) {
+  if (w.err) return NB_OK;
+  NB_TRY(dalloc(&w.err, 4));
+  NB_CUDA(cudaMemset(w.err, 0, 4 * sizeof(unsigned)));
+  NB_CUDA(cudaMallocHost((void**)&w.h_err, 4 * sizeof(unsigned)));
+  NB_TRY(dalloc(&w.bbox, 8));
+  NB_TRY(dalloc(&w.bbox_part, (size_t)kPrepMaxBlocks * 6));
+  NB_TRY(dalloc(&w.bbox_ticket, 4));
+  NB_CUDA(cudaMemset(w.bbox_ticket, 0, 4 * sizeof(unsigned)));
+  NB_TRY(dalloc(&w.eout, 8));
+  NB_TRY(dalloc(&w.eticket, 4));
+  NB_CUDA(cudaMemset(w.eticket, 0, 4 * sizeof(unsigned)));
+  NB_CUDA(cudaMallocHost((void**)&w.h_eout, 8 * sizeof(double)));
+  return NB_OK;
+}
+
+int ws_reserve(Workspace& w, int n, int key_bits) {
+  NB_TRY(ws_basic(w));
+  if (n <= w.cap && key_bits <= w.key_bits) return NB_OK;
+  int cap = n > w.cap ? n : w.cap;
+  int kb = key_bits > w.key_bits ? key_bits : w.key_bits;
+  size_t ksz = kb == 63 ? 8 : 4;
+  size_t ni = cap > 1 ? (size_t)cap - 1 : 1;
+  void* k0 = w.keys;
+  void* k1 = w.keys_alt;
+  if (k0) cudaFree(k0);
+  if (k1) cudaFree(k1);
+  w.keys = w.keys_alt = nullptr;
+  NB_CUDA(cudaMalloc(&w.keys, cap * ksz));
+  NB_CUDA(cudaMalloc(&w.keys_alt, cap * ksz));
+  NB_TRY(dalloc(&w.vals, cap));
+  NB_TRY(dalloc(&w.vals_alt, cap));
+  NB_TRY(dalloc(&w.pos_sorted, cap));
+  NB_TRY(dalloc(&w.nodes, ni));
+  NB_TRY(dalloc(&w.parent, 2 * (size_t)cap));
+  NB_TRY(dalloc(&w.visit, ni));
+  NB_TRY(dalloc(&w.sums, ni));
+  NB_TRY(dalloc(&w.box_lo, ni));
+  NB_TRY(dalloc(&w.box_hi, ni));
+  NB_TRY(dalloc(&w.counts, cap));
+  // defined contents before the first build: in-range indices everywhere
+  NB_CUDA(cudaMemset(w.vals, 0, cap * sizeof(uint32_t)));
+  NB_CUDA(cudaMemset(w.vals_alt, 0, cap * sizeof(uint32_t)));
+  NB_CUDA(cudaMemset(w.parent, 0xff, 2 * (size_t)cap * sizeof(int)));
+  NB_CUDA(cudaMemset(w.nodes, 0, ni * sizeof(Node)));
+  w.status_tiles = (cap + kSortTile - 1) / kSortTile;
+  size_t words = 8 * kSortRadix + 8 + (size_t)8 * w.status_tiles * kSortRadix;
+  NB_TRY(dalloc(&w.hist, words));
+  NB_CUDA(cudaMemset(w.hist, 0, words * sizeof(uint32_t)));
+  w.tile_ctr = w.hist + 8 * kSortRadix;
+  w.status = w.hist + 8 * kSortRadix + 8;
+  w.cap = cap;
+  w.key_bits = kb;
+  return NB_OK;
+}
+
+int ws_reserve_allpairs(Workspace& w, int n, int jsplit) {
+  NB_TRY(ws_basic(w));
+  int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
+  if (npad > w.src_cap) {
+    NB_TRY(dalloc(&w.src, (size_t)npad));   // 2 float4 per pair = npad float4
+    w.src_cap = npad;
+  }
+  size_t need = jsplit > 1 ? (size_t)jsplit * n : 1;
+  if ((int)need > w.part_cap) {
+    NB_TRY(dalloc(&w.part, need));
+    w.part_cap = (int)need;
+  }
+  int itiles = (n + 1023) / 1024 + 1;
+  if (itiles > w.tickets_cap) {
+    NB_TRY(dalloc(&w.tickets, (size_t)itiles));
+    NB_CUDA(cudaMemset(w.tickets, 0, itiles * sizeof(unsigned)));
+    w.tickets_cap = itiles;
+  }
+  return NB_OK;
+}
+
+int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit) {
+  NB_TRY(ws_basic(w));
+  if (blocks * 5 > w.epart_cap) {
+    NB_TRY(dalloc(&w.epart, (size_t)blocks * 5));
+    w.epart_cap = blocks * 5;
+  }
+  size_t need = (size_t)jsplit * n;
+  if (need > (size_t)w.ephi_cap) {
+    NB_TRY(dalloc(&w.ephi, need));
+    w.ephi_cap = (int)need;
+  }
+  return NB_OK;
+}
+
+void ws_free(Workspace& w) {
+  cudaFree(w.keys); cudaFree(w.keys_alt); cudaFree(w.vals); cudaFree(w.vals_alt);
+  cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.parent); cudaFree(w.visit);
+  cudaFree(w.sums); cudaFree(w.box_lo); cudaFree(w.box_hi); cudaFree(w.hist);
+  cudaFree(w.bbox); cudaFree(w.bbox_part); cudaFree(w.bbox_ticket);
+  cudaFree(w.src); cudaFree(w.part); cudaFree(w.tickets); cudaFree(w.epart);
+  cudaFree(w.ephi); cudaFree(w.eout); cudaFree(w.eticket); cudaFree(w.counts);
+  cudaFree(w.err);
+  if (w.h_eout) cudaFreeHost(w.h_eout);
+  if (w.h_err) cudaFreeHost(w.h_err);
+  w = Workspace{};
+}
+
+// ---------------------------------------------------------------------------
+// Parameters
+// ---------------------------------------------------------------------------
+static int check_params(const nb_params* p) {
+  if (!p) return set_error(NB_ERR_INVALID, "params is NULL");
+  if (!(p->eps > 0.f) || !std::isfinite(p->eps))
+    return set_error(NB_ERR_INVALID, "eps must be a finite value > 0");
+  if (!(p->theta >= 0.f) || !std::isfinite(p->theta))
+    return set_error(NB_ERR_INVALID, "theta must be >= 0");
+  if (!std::isfinite(p->dt) || !std::isfinite(p->G))
+    return set_error(NB_ERR_INVALID, "dt and G must be finite");
+  if (p->force != NB_FORCE_NAIVE && p->force != NB_FORCE_BH)
+    return set_error(NB_ERR_INVALID, "force must be NB_FORCE_NAIVE or NB_FORCE_BH");
+  if (p->traverse != NB_TRAVERSE_THREAD && p->traverse != NB_TRAVERSE_WARP)
+    return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
+  if (p->key_bits != 30 && p->key_bits != 63)
+    return set_error(NB_ERR_INVALID, "key_bits must be 30 or 63");
+  return NB_OK;
+}
+
+static int check_n(int n) {
+  if (n <= 0) return set_error(NB_ERR_INVALID, "n must be > 0");
+  if (n >= (1 << 29)) return set_error(NB_ERR_INVALID, "n must be < 2^29");
+  return NB_OK;
+}
+
+static StepArgs make_args(int n, float4* pos, float4* lo, float4* vel,
+                          float4* acc, const nb_params& p) {
+  StepArgs a;
+  a.n = n;
+  a.pos = pos;
+  a.pos_lo = lo;
+  a.vel = vel;
+  a.acc = acc;
+  a.half_dt = 0.5f * p.dt;
+  a.dt = p.dt;
+  a.eps2 = p.eps * p.eps;
+  a.G = p.G;
+  a.theta2 = p.theta * p.theta;
+  a.key_bits = p.key_bits;
+  a.traverse = p.traverse;
+  a.kick_drift = false;
+  a.kick_after = false;
+  a.counts = nullptr;
+  return a;
+}
+
+// Phase event recorder: when `ev` is non-null, records an event after each
+// phase into ev[phase].
+struct PhaseMarks {
+  cudaEvent_t start = nullptr;
+  cudaEvent_t mark[NB_PHASES] = {};
+  bool used[NB_PHASES] = {};
+};
+
+static int mark(PhaseMarks* pm, int phase, cudaStream_t st) {
+  if (!pm) return NB_OK;
+  NB_CUDA(cudaEventRecord(pm->mark[phase], st));
+  pm->used[phase] = true;
+  return NB_OK;
+}
+
+// The whole force evaluation (plus the optional fused kick / drift / kick).
+// n < 2 with Barnes-Hut writes zeros as src/forces_bh.cu:466-469 does.
+static int enqueue_forces(Workspace& w, const StepArgs& a, int force,
+                          cudaStream_t st, PhaseMarks* pm) {
+  if (pm) NB_CUDA(cudaEventRecord(pm->start, st));
+  if (force == NB_FORCE_BH && a.n < 2) {
+    if (a.kick_drift) NB_TRY(launch_prep(w, a, false, false, st));
+    NB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float4) * a.n, st));
+    return mark(pm, NB_PHASE_WALK, st);
+  }
+  if (force == NB_FORCE_NAIVE) {
+    NB_TRY(ws_reserve_allpairs(w, a.n, allpairs_geometry(a.n).jsplit));
+    NB_TRY(launch_prep(w, a, false, true, st));
+    NB_TRY(mark(pm, NB_PHASE_PREP, st));
+    NB_TRY(launch_allpairs(w, a, st));
+    return mark(pm, NB_PHASE_WALK, st);
+  }
+  NB_TRY(ws_reserve(w, a.n, a.key_bits));
+  NB_TRY(launch_prep(w, a, true, false, st));
+  NB_TRY(mark(pm, NB_PHASE_PREP, st));
+  NB_TRY(launch_morton(w, a, st));
+  NB_TRY(mark(pm, NB_PHASE_MORTON, st));
+  NB_TRY(launch_sort(w, a, st));
+  NB_TRY(mark(pm, NB_PHASE_SORT, st));
+  NB_TRY(launch_build(w, a, st));
+  NB_TRY(mark(pm, NB_PHASE_BUILD, st));
+  NB_TRY(launch_com(w, a, st));
+  NB_TRY(mark(pm, NB_PHASE_COM, st));
+  NB_TRY(launch_walk(w, a, st));
+  return mark(pm, NB_PHASE_WALK, st);
+}
+
+static int check_device_error(Workspace& w, cudaStream_t st) {
+  if (!w.err) return NB_OK;
+  NB_CUDA(cudaMemcpyAsync(w.h_err, w.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  unsigned e = *w.h_err;
+  if (e) {
+    NB_CUDA(cudaMemsetAsync(w.err, 0, sizeof(unsigned), st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    std::string m = "device error word 0x";
+    char buf[16];
+    std::snprintf(buf, sizeof(buf), "%x", e);
+    m += buf;
+    if (e & NB_DEVERR_STACK) m += " (tree walk stack overflow)";
+    if (e & NB_DEVERR_SORT) m += " (radix sort look-back wait limit)";
+    if (e & NB_DEVERR_WAIT) m += " (bulk-copy barrier wait limit)";
+    if (e & NB_DEVERR_QUEUE) m += " (work-queue wait limit)";
+    return set_error(NB_ERR_DEVICE, m);
+  }
+  return NB_OK;
+}
+
+}  // namespace nb
+
+using namespace nb;
+
+// ===========================================================================
+// Simulation handle
+// ===========================================================================
+struct nb_sim {
+  int n = 0;
+  nb_params p{};
+  cudaStream_t stream = nullptr;
+  float4* pos = nullptr;
+  float4* pos_lo = nullptr;
+  float4* vel = nullptr;
+  float4* acc = nullptr;
+  Workspace ws;
+  bool primed = false;
+  // graphs
+  bool use_graphs = true;
+  cudaGraphExec_t graph = nullptr;
+  bool graph_valid = false;
+  // timing
+  bool timing = false;
+  std::vector<PhaseMarks*> pending;
+  std::vector<PhaseMarks*> pool;
+  double phase_ms[NB_PHASES] = {};
+  long timed_steps = 0;
+  double force_ms = 0.0;
+  long force_calls = 0;
+  cudaEvent_t slots[16] = {};
+  void* flush_buf = nullptr;
+  size_t flush_bytes = 0;
+};
+
+static void sim_free(nb_sim* s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (auto* pm : s->pending) s->pool.push_back(pm);
+  for (auto* pm : s->pool) {
+    cudaEventDestroy(pm->start);
+    for (int i = 0; i < NB_PHASES; ++i) cudaEventDestroy(pm->mark[i]);
+    delete pm;
+  }
+  for (auto& e : s->slots)
+    if (e) cudaEventDestroy(e);
+  cudaFree(s->flush_buf);
+  cudaFree(s->pos);
+  cudaFree(s->pos_lo);
+  cudaFree(s->vel);
+  cudaFree(s->acc);
+  ws_free(s->ws);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+static int get_marks(nb_sim* s, PhaseMarks** out) {
+  if (!s->pool.empty()) {
+    *out = s->pool.back();
+    s->pool.pop_back();
+  } else {
+    PhaseMarks* pm = new PhaseMarks();
+    NB_CUDA(cudaEventCreate(&pm->start));
+    for (int i = 0; i < NB_PHASES; ++i) NB_CUDA(cudaEventCreate(&pm->mark[i]));
+    *out = pm;
+  }
+  for (int i = 0; i < NB_PHASES; ++i) (*out)->used[i] = false;
+  s->pending.push_back(*out);
+  return NB_OK;
+}
+
+// Folds the recorded phase events into the accumulators (synchronises).
+static int collect_timing(nb_sim* s) {
+  if (s->pending.empty()) return NB_OK;
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  for (PhaseMarks* pm : s->pending) {
+    cudaEvent_t prev = pm->start;
+    double total = 0.0;
+    bool any = false;
+    for (int i = 0; i < NB_PHASES; ++i) {
+      if (!pm->used[i]) continue;
+      float ms = 0.f;
+      NB_CUDA(cudaEventElapsedTime(&ms, prev, pm->mark[i]));
+      s->phase_ms[i] += ms;
+      if (i != NB_PHASE_ENERGY) total += ms;
+      prev = pm->mark[i];
+      any = true;
+    }
+    if (any && !pm->used[NB_PHASE_ENERGY]) {
+      s->force_ms += total;
+      ++s->force_calls;
+      ++s->timed_steps;
+    }
+    s->pool.push_back(pm);
+  }
+  s->pending.clear();
+  return NB_OK;
+}
+
+namespace nb {
+int sim_view(nb_sim* s, SimView* v) {
+  if (!s || !v) return set_error(NB_ERR_INVALID, "NULL argument");
+  v->n = s->n;
+  v->stream = s->stream;
+  v->pos = s->pos;
+  v->vel = s->vel;
+  v->ws = &s->ws;
+  v->p = s->p;
+  return NB_OK;
+}
+}  // namespace nb
+
+static StepArgs sim_args(nb_sim* s) {
+  return make_args(s->n, s->pos, s->p.compensated ? s->pos_lo : nullptr,
+                   s->vel, s->acc, s->p);
+}
+
+// a(x) into s->acc, no kick / drift.
+static int sim_forces(nb_sim* s, int* counts) {
+  StepArgs a = sim_args(s);
+  a.counts = counts;
+  PhaseMarks* pm = nullptr;
+  if (s->timing) NB_TRY(get_marks(s, &pm));
+  NB_TRY(enqueue_forces(s->ws, a, s->p.force, s->stream, pm));
+  s->primed = true;
+  return NB_OK;
+}
+
+static int sim_step_eager(nb_sim* s, PhaseMarks* pm) {
+  StepArgs a = sim_args(s);
+  a.kick_drift = true;
+  a.kick_after = true;
+  return enqueue_forces(s->ws, a, s->p.force, s->stream, pm);
+}
+
+static int sim_capture(nb_sim* s) {
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  s->graph_valid = false;
+  // reserve first so no allocation happens during capture
+  if (s->p.force == NB_FORCE_BH)
+    NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
+  else
+    NB_TRY(ws_reserve_allpairs(s->ws, s->n, allpairs_geometry(s->n).jsplit));
+  cudaGraph_t g = nullptr;
+  NB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = sim_step_eager(s, nullptr);
+  cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (rc != NB_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess)
+    return set_error(NB_ERR_CUDA, std::string("cudaStreamEndCapture: ") +
+                                      cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&s->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return set_error(NB_ERR_CUDA, std::string("cudaGraphInstantiate: ") +
+                                      cudaGetErrorString(e));
+  s->graph_valid = true;
+  return NB_OK;
+}
+
+extern "C" {
+
+void nb_params_default(nb_params* p) {
+  if (!p) return;
+  p->dt = 0.01f;
+  p->eps = 0.05f;
+  p->G = 1.0f;
+  p->theta = 0.5f;
+  p->force = NB_FORCE_NAIVE;
+  p->traverse = NB_TRAVERSE_THREAD;
+  p->key_bits = 30;
+  p->compensated = 1;
+}
+
+const char* nb_last_error(void) { return nb::last_error(); }
+int nb_version(void) { return 100; }
+
+int nb_device_count(int* out) {
+  if (!out) return set_error(NB_ERR_INVALID, "out is NULL");
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c = 0;
+  }
+  *out = c;
+  return NB_OK;
+}
+
+int nb_set_device(int device) {
+  NB_CUDA(cudaSetDevice(device));
+  return NB_OK;
+}
+
+int nb_alloc_pinned(size_t bytes, void** out) {
+  if (!out) return set_error(NB_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  cudaError_t e = cudaMallocHost(out, bytes ? bytes : 1);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return set_error(NB_ERR_NOMEM, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+  }
+  return NB_OK;
+}
+
+int nb_free_pinned(void* p) {
+  if (p) NB_CUDA(cudaFreeHost(p));
+  return NB_OK;
+}
+
+int nb_measure_fp32_peak(double* tflops_scalar, double* tflops_packed) {
+  if (!tflops_scalar || !tflops_packed) return set_error(NB_ERR_INVALID, "NULL argument");
+  return measure_fp32_peak(tflops_scalar, tflops_packed);
+}
+
+int nb_flush_l2(nb_sim* s, size_t bytes) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  if (bytes > s->flush_bytes) {
+    cudaFree(s->flush_buf);
+    s->flush_buf = nullptr;
+    s->flush_bytes = 0;
+    NB_CUDA(cudaMalloc(&s->flush_buf, bytes));
+    s->flush_bytes = bytes;
+  }
+  return launch_flush(s->flush_buf, bytes, s->stream);
+}
+
+int nb_sim_create(int n, const float* pos4, const float* vel4,
+                  const nb_params* p, nb_sim** out) {
+  if (!out) return set_error(NB_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  if (!pos4 || !vel4) return set_error(NB_ERR_INVALID, "pos4 / vel4 is NULL");
+  nb_sim* s = new nb_sim();
+  s->n = n;
+  s->p = *p;
+  int rc = NB_OK;
+  do {
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { rc = set_error(NB_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e)); break; }
+    if ((rc = dalloc(&s->pos, n)) != NB_OK) break;
+    if ((rc = dalloc(&s->pos_lo, n)) != NB_OK) break;
+    if ((rc = dalloc(&s->vel, n)) != NB_OK) break;
+    if ((rc = dalloc(&s->acc, n)) != NB_OK) break;
+    if ((rc = ws_basic(s->ws)) != NB_OK) break;
+    rc = nb_set_state(s, pos4, vel4);
+  } while (0);
+  if (rc != NB_OK) {
+    std::string keep = nb::last_error();
+    sim_free(s);
+    return set_error(rc, keep);
+  }
+  *out = s;
+  return NB_OK;
+}
+
+int nb_sim_destroy(nb_sim* s) {
+  sim_free(s);
+  return NB_OK;
+}
+
+int nb_sim_n(const nb_sim* s, int* n) {
+  if (!s || !n) return set_error(NB_ERR_INVALID, "NULL argument");
+  *n = s->n;
+  return NB_OK;
+}
+
+int nb_set_params(nb_sim* s, const nb_params* p) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_TRY(check_params(p));
+  bool changes_forces = p->force != s->p.force || p->eps != s->p.eps ||
+                        p->G != s->p.G || p->theta != s->p.theta ||
+                        p->traverse != s->p.traverse ||
+                        p->key_bits != s->p.key_bits;
+  if (p->compensated && !s->p.compensated)
+    NB_CUDA(cudaMemsetAsync(s->pos_lo, 0, sizeof(float4) * s->n, s->stream));
+  s->p = *p;
+  s->graph_valid = false;
+  if (changes_forces) s->primed = false;
+  return NB_OK;
+}
+
+int nb_get_params(const nb_sim* s, nb_params* p) {
+  if (!s || !p) return set_error(NB_ERR_INVALID, "NULL argument");
+  *p = s->p;
+  return NB_OK;
+}
+
+int nb_set_state(nb_sim* s, const float* pos4, const float* vel4) {
+  if (!s || !pos4 || !vel4) return set_error(NB_ERR_INVALID, "NULL argument");
+  size_t b = sizeof(float4) * s->n;
+  NB_CUDA(cudaMemcpyAsync(s->pos, pos4, b, cudaMemcpyHostToDevice, s->stream));
+  NB_CUDA(cudaMemcpyAsync(s->vel, vel4, b, cudaMemcpyHostToDevice, s->stream));
+  NB_CUDA(cudaMemsetAsync(s->pos_lo, 0, b, s->stream));
+  // the reference ignores vel.w; keep it as given
+  s->primed = false;
+  return NB_OK;
+}
+
+static int download(nb_sim* s, float* dst, const float4* src) {
+  if (!s || !dst) return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_CUDA(cudaMemcpyAsync(dst, src, sizeof(float4) * s->n,
+                          cudaMemcpyDeviceToHost, s->stream));
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s->ws, s->stream);
+}
+
+int nb_set_state_acc(nb_sim* s, const float* pos4, const float* vel4,
+                     const float* acc4) {
+  if (!s || !acc4) return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_TRY(nb_set_state(s, pos4, vel4));
+  NB_CUDA(cudaMemcpyAsync(s->acc, acc4, sizeof(float4) * s->n,
+                          cudaMemcpyHostToDevice, s->stream));
+  s->primed = true;
+  return NB_OK;
+}
+
+int nb_get_accelerations(nb_sim* s, float* acc4) { return download(s, acc4, s ? s->acc : nullptr); }
+int nb_get_positions(nb_sim* s, float* pos4) { return download(s, pos4, s ? s->pos : nullptr); }
+int nb_get_velocities(nb_sim* s, float* vel4) { return download(s, vel4, s ? s->vel : nullptr); }
+int nb_get_position_lo(nb_sim* s, float* lo4) { return download(s, lo4, s ? s->pos_lo : nullptr); }
+
+int nb_compute_forces(nb_sim* s, float* acc4) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_TRY(sim_forces(s, nullptr));
+  if (acc4) return download(s, acc4, s->acc);
+  return NB_OK;
+}
+
+int nb_step(nb_sim* s, int nsteps) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  if (nsteps < 0) return set_error(NB_ERR_INVALID, "nsteps must be >= 0");
+  if (nsteps == 0) return NB_OK;
+  if (!s->primed) NB_TRY(sim_forces(s, nullptr));   // a(x0), src/main.cu:184
+  for (int k = 0; k < nsteps; ++k) {
+    if (s->timing) {
+      PhaseMarks* pm = nullptr;
+      NB_TRY(get_marks(s, &pm));
+      NB_TRY(sim_step_eager(s, pm));
+      continue;
+    }
+    if (s->use_graphs) {
+      if (!s->graph_valid) NB_TRY(sim_capture(s));
+      NB_CUDA(cudaGraphLaunch(s->graph, s->stream));
+    } else {
+      NB_TRY(sim_step_eager(s, nullptr));
+    }
+  }
+  return NB_OK;
+}
+
+int nb_sync(nb_sim* s) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s->ws, s->stream);
+}
+
+int nb_energy(nb_sim* s, double* e3, double* mom3) {
+  if (!s || !e3) return set_error(NB_ERR_INVALID, "NULL argument");
+  PhaseMarks* pm = nullptr;
+  if (s->timing) {
+    NB_TRY(get_marks(s, &pm));
+    NB_CUDA(cudaEventRecord(pm->start, s->stream));
+  }
+  NB_TRY(launch_energy(s->ws, s->n, s->pos, s->vel, s->p.eps * s->p.eps, s->p.G,
+                       s->stream));
+  if (pm) NB_TRY(mark(pm, NB_PHASE_ENERGY, s->stream));
+  NB_CUDA(cudaMemcpyAsync(s->ws.h_eout, s->ws.eout, 6 * sizeof(double),
+                          cudaMemcpyDeviceToHost, s->stream));
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  NB_TRY(check_device_error(s->ws, s->stream));
+  e3[0] = s->ws.h_eout[0];
+  e3[1] = s->ws.h_eout[1];
+  e3[2] = s->ws.h_eout[2];
+  if (mom3) {
+    mom3[0] = s->ws.h_eout[3];
+    mom3[1] = s->ws.h_eout[4];
+    mom3[2] = s->ws.h_eout[5];
+  }
+  return NB_OK;
+}
+
+int nb_set_timing(nb_sim* s, int enable) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  s->timing = enable != 0;
+  return NB_OK;
+}
+
+int nb_force_timing(nb_sim* s, double* ms_total, long* calls) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_TRY(collect_timing(s));
+  if (ms_total) *ms_total = s->force_ms;
+  if (calls) *calls = s->force_calls;
+  return NB_OK;
+}
+
+int nb_reset_timing(nb_sim* s) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_TRY(collect_timing(s));
+  for (double& v : s->phase_ms) v = 0.0;
+  s->timed_steps = 0;
+  s->force_ms = 0.0;
+  s->force_calls = 0;
+  return NB_OK;
+}
+
+int nb_phase_times(nb_sim* s, double* ms, long* calls) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  NB_TRY(collect_timing(s));
+  if (ms)
+    for (int i = 0; i < NB_PHASES; ++i) ms[i] = s->phase_ms[i];
+  if (calls) *calls = s->timed_steps;
+  return NB_OK;
+}
+
+int nb_record(nb_sim* s, int slot) {
+  if (!s || slot < 0 || slot >= 16) return set_error(NB_ERR_INVALID, "bad slot");
+  if (!s->slots[slot]) NB_CUDA(cudaEventCreate(&s->slots[slot]));
+  NB_CUDA(cudaEventRecord(s->slots[slot], s->stream));
+  return NB_OK;
+}
+
+int nb_elapsed_ms(nb_sim* s, int a, int b, double* ms) {
+  if (!s || !ms || a < 0 || b < 0 || a >= 16 || b >= 16 || !s->slots[a] ||
+      !s->slots[b])
+    return set_error(NB_ERR_INVALID, "bad slot");
+  NB_CUDA(cudaEventSynchronize(s->slots[b]));
+  float f = 0.f;
+  NB_CUDA(cudaEventElapsedTime(&f, s->slots[a], s->slots[b]));
+  *ms = f;
+  return NB_OK;
+}
+
+int nb_set_graphs(nb_sim* s, int enable) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  s->use_graphs = enable != 0;
+  s->graph_valid = false;
+  return NB_OK;
+}
+
+int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
+                  int32_t* children, int32_t* parent, float* com4,
+                  float* size2) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  if (s->n < 2) return set_error(NB_ERR_INVALID, "n must be >= 2 for a tree");
+  nb_params bh = s->p;
+  bh.force = NB_FORCE_BH;
+  StepArgs a = make_args(s->n, s->pos, nullptr, s->vel, s->acc, bh);
+  float4* tmp = nullptr;
+  NB_TRY(dalloc(&tmp, s->n));
+  a.acc = tmp;   // leave the simulation's a(x) untouched
+  int rc = enqueue_forces(s->ws, a, NB_FORCE_BH, s->stream, nullptr);
+  if (rc == NB_OK) {
+    cudaStream_t st = s->stream;
+    const int n = s->n, ni = n - 1;
+    std::vector<unsigned char> kbuf((size_t)n * 8);
+    size_t ksz = s->p.key_bits == 63 ? 8 : 4;
+    cudaMemcpyAsync(kbuf.data(), s->ws.keys, n * ksz, cudaMemcpyDeviceToHost, st);
+    if (perm) cudaMemcpyAsync(perm, s->ws.vals, n * 4, cudaMemcpyDeviceToHost, st);
+    std::vector<Node> nodes(ni);
+    cudaMemcpyAsync(nodes.data(), s->ws.nodes, ni * sizeof(Node), cudaMemcpyDeviceToHost, st);
+    if (parent) cudaMemcpyAsync(parent, s->ws.parent, (2 * (size_t)n - 1) * 4, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = set_error(NB_ERR_CUDA, cudaGetErrorString(e));
+    if (rc == NB_OK) rc = check_device_error(s->ws, st);
+    if (rc == NB_OK) {
+      for (int i = 0; i < n && keys_sorted; ++i)
+        keys_sorted[i] = ksz == 8 ? ((uint64_t*)kbuf.data())[i]
+                                  : (uint64_t)((uint32_t*)kbuf.data())[i];
+      for (int i = 0; i < ni; ++i) {
+        if (children) { children[2 * i] = nodes[i].left; children[2 * i + 1] = nodes[i].right; }
+        if (com4) { com4[4 * i] = nodes[i].com.x; com4[4 * i + 1] = nodes[i].com.y;
+                    com4[4 * i + 2] = nodes[i].com.z; com4[4 * i + 3] = nodes[i].com.w; }
+        if (size2) size2[i] = nodes[i].size2;
+      }
+    }
+  }
+  cudaFree(tmp);
+  return rc;
+}
+
+int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts) {
+  if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
+  int* dcounts = nullptr;
+  if (counts && s->p.force == NB_FORCE_BH && s->n >= 2) {
+    NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
+    dcounts = s->ws.counts;
+  }
+  NB_TRY(sim_forces(s, dcounts));
+  if (acc4) NB_TRY(download(s, acc4, s->acc));
+  if (counts) {
+    if (dcounts) {
+      std::vector<int> cs(s->n);
+      std::vector<uint32_t> perm(s->n);
+      NB_CUDA(cudaMemcpyAsync(cs.data(), dcounts, s->n * 4, cudaMemcpyDeviceToHost, s->stream));
+      NB_CUDA(cudaMemcpyAsync(perm.data(), s->ws.vals, s->n * 4, cudaMemcpyDeviceToHost, s->stream));
+      NB_CUDA(cudaStreamSynchronize(s->stream));
+      for (int t = 0; t < s->n; ++t) counts[perm[t]] = cs[t];
+    } else {
+      for (int i = 0; i < s->n; ++i) counts[i] = s->n;   // all-pairs: n each
+    }
+  }
+  return NB_OK;
+}
+
+int nb_compare_forces(nb_sim* s, double* max_rel, double* mean_rel) {
+  if (!s || !max_rel || !mean_rel) return set_error(NB_ERR_INVALID, "NULL argument");
+  const int n = s->n;
+  std::vector<float> a(4 * (size_t)n), b(4 * (size_t)n);
+  nb_params keep = s->p;
+  nb_params pn = keep, pb = keep;
+  pn.force = NB_FORCE_NAIVE;
+  pb.force = NB_FORCE_BH;
+  int rc = nb_set_params(s, &pn);
+  if (rc == NB_OK) rc = nb_compute_forces(s, a.data());
+  if (rc == NB_OK) rc = nb_set_params(s, &pb);
+  if (rc == NB_OK) rc = nb_compute_forces(s, b.data());
+  nb_set_params(s, &keep);
+  if (rc != NB_OK) return rc;
+  double mx = 0.0, sum = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double dx = (double)a[4 * i] - b[4 * i], dy = (double)a[4 * i + 1] - b[4 * i + 1],
+           dz = (double)a[4 * i + 2] - b[4 * i + 2];
+    double an = std::sqrt((double)a[4 * i] * a[4 * i] + (double)a[4 * i + 1] * a[4 * i + 1] +
+                          (double)a[4 * i + 2] * a[4 * i + 2]);
+    double rel = std::sqrt(dx * dx + dy * dy + dz * dz) / (an + 1e-30);
+    sum += rel;
+    if (rel > mx) mx = rel;
+  }
+  *max_rel = mx;
+  *mean_rel = sum / n;
+  return NB_OK;
+}
+
+// ===========================================================================
+// Device-pointer drop-ins
+// ===========================================================================
+}  // extern "C"
+
+struct nb_workspace {
+  Workspace ws;
+};
+
+extern "C" {
+
+int nb_workspace_create(nb_workspace** out) {
+  if (!out) return set_error(NB_ERR_INVALID, "out is NULL");
+  *out = new nb_workspace();
+  return NB_OK;
+}
+
+int nb_workspace_destroy(nb_workspace* w) {
+  if (!w) return NB_OK;
+  cudaDeviceSynchronize();
+  ws_free(w->ws);
+  delete w;
+  return NB_OK;
+}
+
+int nb_compute_forces_dev(nb_workspace* w, int n, const float* d_pos4,
+                          float* d_acc4, const nb_params* p, void* stream) {
+  if (!w || !d_pos4 || !d_acc4) return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  StepArgs a = make_args(n, (float4*)d_pos4, nullptr, nullptr, (float4*)d_acc4, *p);
+  return enqueue_forces(w->ws, a, p->force, (cudaStream_t)stream, nullptr);
+}
+
+int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_vel4,
+                         float* d_acc4, const nb_params* p, void* stream) {
+  if (!w || !d_pos4 || !d_vel4 || !d_acc4)
+    return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  StepArgs a = make_args(n, (float4*)d_pos4, nullptr, (float4*)d_vel4,
+                         (float4*)d_acc4, *p);
+  a.kick_drift = true;
+  a.kick_after = true;
+  return enqueue_forces(w->ws, a, p->force, (cudaStream_t)stream, nullptr);
+}
+
+int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,
+                        const float* d_vel4, const nb_params* p, double* e3,
+                        void* stream) {
+  if (!w || !d_pos4 || !d_vel4 || !e3) return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  cudaStream_t st = (cudaStream_t)stream;
+  NB_TRY(launch_energy(w->ws, n, (const float4*)d_pos4, (const float4*)d_vel4,
+                       p->eps * p->eps, p->G, st));
+  NB_CUDA(cudaMemcpyAsync(w->ws.h_eout, w->ws.eout, 6 * sizeof(double),
+                          cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  NB_TRY(check_device_error(w->ws, st));
+  e3[0] = w->ws.h_eout[0];
+  e3[1] = w->ws.h_eout[1];
+  e3[2] = w->ws.h_eout[2];
+  return NB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,386 @@
+// Tiled all-pairs softened gravity (src/forces.cu:17-60) and the all-pairs
+// energy diagnostic (src/integrator.cu:43-110), written for sm_100a:
+//
+// * j-particle tiles of 512 sources (8 KB) move global -> shared memory by
+//   TMA bulk copies (cp.async.bulk, no multicast) into a 3-stage ring of
+//   mbarrier-tracked buffers; one elected thread issues the copies.
+// * Sources are packed in pairs, (x0,x1,y0,y1)(z0,z1,m0,m1), so one 128-bit
+//   shared load gives two sources per coordinate and the pair math runs on
+//   Blackwell's packed FP32 pipe (fma/add/mul .f32x2): 12 packed ops and two
+//   MUFU rsqrt per two interactions.
+// * Each thread holds K targets; even and odd sources accumulate in the two
+//   halves of a packed accumulator and are added at the end (FP32).
+// * Small n splits the source range over `jsplit` CTAs per target tile; the
+//   last CTA of a tile (ticket) sums the partials in fixed order, so results
+//   are deterministic.  The leapfrog's closing kick is fused in the epilogue.
+#include "nb_internal.cuh"
+
+namespace nb {
+
+typedef unsigned long long f2;   // two packed floats
+
+__device__ __forceinline__ f2 pk2(float a, float b) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(f2 r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// --- mbarrier / bulk-copy helpers -----------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(count) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src,
+                                          uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes),
+      "r"(smem_u32(bar)) : "memory");
+}
+// Bounded wait on a phase parity; false when the limit is reached.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 24); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;"
+        " selp.u32 %0, 1, 0, p; }"
+        : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+constexpr int kStages = 3;
+constexpr int kTileF4 = kSrcTile;                 // float4 per tile (2 per pair)
+constexpr uint32_t kTileBytes = kTileF4 * 16u;   // 8 KB
+
+struct APArgs {
+  int n;
+  const float4* __restrict__ pos;
+  const float4* __restrict__ src;   // packed sources, npad particles
+  int npad;
+  int jsplit;
+  int jchunk;                       // particles per j-chunk (multiple of tile)
+  float eps2, G, half_dt;
+  float4* acc;
+  float4* vel;                      // closing kick or nullptr
+  float4* part;                     // [jsplit][n] partials
+  unsigned* tickets;                // [itiles]
+  unsigned* err;
+};
+
+template <int THREADS, int K>
+__global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
+  __shared__ __align__(128) float4 s_tile[kStages][kTileF4];
+  __shared__ __align__(8) uint64_t s_bar[kStages];
+  __shared__ bool s_last;
+  const int tid = threadIdx.x;
+  const int ibase = blockIdx.x * THREADS * K;
+  const int j0 = blockIdx.y * a.jchunk;
+  const int j1 = min(j0 + a.jchunk, a.npad);
+  const int ntiles = (j1 - j0) / kSrcTile;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&s_bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < kStages && s < ntiles; ++s)
+      bulk_load(s_tile[s], a.src + 2 * ((j0 + s * kSrcTile) / 2), kTileBytes,
+                &s_bar[s]);
+  }
+
+  f2 nx[K], ny[K], nz[K], ax[K], ay[K], az[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    int i = ibase + k * THREADS + tid;
+    float4 p = a.pos[i < a.n ? i : a.n - 1];
+    nx[k] = pk2(-p.x, -p.x);
+    ny[k] = pk2(-p.y, -p.y);
+    nz[k] = pk2(-p.z, -p.z);
+    ax[k] = ay[k] = az[k] = 0ull;
+  }
+  const f2 e2 = pk2(a.eps2, a.eps2);
+
+  bool ok = true;
+  for (int t = 0; t < ntiles; ++t) {
+    const int s = t % kStages;
+    if (!mbar_wait(&s_bar[s], (uint32_t)((t / kStages) & 1))) {
+      ok = false;
+      break;
+    }
+    const ulonglong2* tile = reinterpret_cast<const ulonglong2*>(s_tile[s]);
+#pragma unroll 4
+    for (int q = 0; q < kSrcTile / 2; ++q) {
+      const ulonglong2 A = tile[2 * q];       // (x0,x1) (y0,y1)
+      const ulonglong2 B = tile[2 * q + 1];   // (z0,z1) (m0,m1)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        f2 dx = add2(A.x, nx[k]);
+        f2 dy = add2(A.y, ny[k]);
+        f2 dz = add2(B.x, nz[k]);
+        f2 r2 = fma2(dz, dz, e2);
+        r2 = fma2(dy, dy, r2);
+        r2 = fma2(dx, dx, r2);
+        float r0, r1;
+        up2(r2, r0, r1);
+        f2 inv = pk2(mufu_rsqrt(r0), mufu_rsqrt(r1));
+        f2 w = mul2(inv, B.y);
+        f2 i2 = mul2(inv, inv);
+        f2 f = mul2(w, i2);
+        ax[k] = fma2(dx, f, ax[k]);
+        ay[k] = fma2(dy, f, ay[k]);
+        az[k] = fma2(dz, f, az[k]);
+      }
+    }
+    __syncthreads();   // every thread is done with stage s
+    if (tid == 0 && t + kStages < ntiles)
+      bulk_load(s_tile[s], a.src + 2 * ((j0 + (t + kStages) * kSrcTile) / 2),
+                kTileBytes, &s_bar[s]);
+  }
+  if (!ok) {
+    if (tid == 0) raise_err(a.err, NB_DEVERR_WAIT);
+    return;
+  }
+
+  float3 res[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    float u, v;
+    up2(ax[k], u, v); res[k].x = u + v;
+    up2(ay[k], u, v); res[k].y = u + v;
+    up2(az[k], u, v); res[k].z = u + v;
+  }
+
+  if (a.jsplit > 1) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      int i = ibase + k * THREADS + tid;
+      if (i < a.n)
+        a.part[(size_t)blockIdx.y * a.n + i] =
+            make_float4(res[k].x, res[k].y, res[k].z, 0.f);
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      unsigned tk = atomicAdd(&a.tickets[blockIdx.x], 1u);
+      s_last = tk == (unsigned)a.jsplit - 1u;
+      if (s_last) a.tickets[blockIdx.x] = 0u;   // ready for the next launch
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      int i = ibase + k * THREADS + tid;
+      float3 sum = make_float3(0.f, 0.f, 0.f);
+      if (i < a.n) {
+        for (int js = 0; js < a.jsplit; ++js) {
+          float4 p = __ldcg(&a.part[(size_t)js * a.n + i]);
+          sum.x += p.x; sum.y += p.y; sum.z += p.z;
+        }
+      }
+      res[k] = sum;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    int i = ibase + k * THREADS + tid;
+    if (i >= a.n) continue;
+    float4 acc = make_float4(a.G * res[k].x, a.G * res[k].y, a.G * res[k].z, 0.f);
+    a.acc[i] = acc;
+    if (a.vel) {
+      float4 v = a.vel[i];
+      v.x = __fmaf_rn(a.half_dt, acc.x, v.x);
+      v.y = __fmaf_rn(a.half_dt, acc.y, v.y);
+      v.z = __fmaf_rn(a.half_dt, acc.z, v.z);
+      a.vel[i] = v;
+    }
+  }
+}
+
+// Geometry: 256 threads x 4 targets per CTA; the source range is split so the
+// grid fills the 148 SMs (two CTAs each) several times over.
+APGeom allpairs_geometry(int n) {
+  APGeom g;
+  g.threads = 256;
+  g.k = 4;
+  const int per = g.threads * g.k;
+  g.itiles = (n + per - 1) / per;
+  const int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
+  const int jtiles = npad / kSrcTile;
+  const int target = 148 * 2 * 4;   // CTAs wanted in flight over the launch
+  int js = (target + g.itiles - 1) / g.itiles;
+  if (js > jtiles) js = jtiles;
+  if (js < 1) js = 1;
+  // round the chunk to whole tiles and recompute the split it implies
+  int jt_per = (jtiles + js - 1) / js;
+  g.jsplit = (jtiles + jt_per - 1) / jt_per;
+  return g;
+}
+
+int launch_allpairs(Workspace& w, const StepArgs& s, cudaStream_t st) {
+  APGeom g = allpairs_geometry(s.n);
+  NB_TRY(ws_reserve_allpairs(w, s.n, g.jsplit));
+  APArgs a;
+  a.n = s.n;
+  a.pos = s.pos;
+  a.src = w.src;
+  a.npad = (s.n + kSrcTile - 1) / kSrcTile * kSrcTile;
+  a.jsplit = g.jsplit;
+  const int jtiles = a.npad / kSrcTile;
+  a.jchunk = (jtiles + g.jsplit - 1) / g.jsplit * kSrcTile;
+  a.eps2 = s.eps2;
+  a.G = s.G;
+  a.half_dt = s.half_dt;
+  a.acc = s.acc;
+  a.vel = s.kick_after ? s.vel : nullptr;
+  a.part = w.part;
+  a.tickets = w.tickets;
+  a.err = w.err;
+  dim3 grid(g.itiles, g.jsplit);
+  k_allpairs<256, 4><<<grid, 256, 0, st>>>(a);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Energy.  PE = -1/2 G sum_i m_i (phi_i - self_i), phi_i = sum_j m_j
+// rsqrt(r_ij^2 + eps^2) including j == i (removed again with the same float
+// rsqrt(eps^2) the loop used for it).  Pair math in FP32, per-tile partial
+// sums converted to FP64; KE, PE and momentum reduced in FP64 in a fixed
+// order (block partials, then the last block).
+// ---------------------------------------------------------------------------
+constexpr int kEThreads = 256;
+constexpr int kETile = 256;
+
+__global__ void __launch_bounds__(kEThreads) k_energy_phi(
+    const float4* __restrict__ pos, int n, float eps2, int jchunk,
+    double* __restrict__ phi_part) {
+  __shared__ float4 s_src[kETile];
+  const int i = blockIdx.x * kEThreads + threadIdx.x;
+  const float4 bi = pos[i < n ? i : n - 1];
+  const int j0 = blockIdx.y * jchunk;
+  const int j1 = min(j0 + jchunk, n);
+  double phi = 0.0;
+  for (int jt = j0; jt < j1; jt += kETile) {
+    int j = jt + threadIdx.x;
+    s_src[threadIdx.x] = j < j1 ? pos[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    float acc = 0.f;
+#pragma unroll 8
+    for (int q = 0; q < kETile; ++q) {
+      float4 s = s_src[q];
+      float dx = s.x - bi.x, dy = s.y - bi.y, dz = s.z - bi.z;
+      float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+      acc = fmaf(s.w, mufu_rsqrt(__fadd_rn(r2, eps2)), acc);
+    }
+    phi += (double)acc;
+    __syncthreads();
+  }
+  if (i < n) phi_part[(size_t)blockIdx.y * n + i] = phi;
+}
+
+__global__ void __launch_bounds__(kEThreads) k_energy_reduce(
+    const float4* __restrict__ pos, const float4* __restrict__ vel, int n,
+    float eps2, float G, int jsplit, const double* __restrict__ phi_part,
+    double* __restrict__ epart, unsigned* ticket, double* out) {
+  __shared__ double s_r[kEThreads / 32][5];
+  __shared__ bool s_last;
+  double r[5] = {0, 0, 0, 0, 0};   // KE, PE, Px, Py, Pz
+  const double self_inv = (double)mufu_rsqrt(eps2);
+  for (int i = blockIdx.x * kEThreads + threadIdx.x; i < n;
+       i += gridDim.x * kEThreads) {
+    float4 p = pos[i];
+    float4 v = vel[i];
+    double m = (double)p.w;
+    double phi = 0.0;
+    for (int js = 0; js < jsplit; ++js) phi += phi_part[(size_t)js * n + i];
+    double self = (double)__fmul_rn(p.w, (float)self_inv);
+    r[0] += 0.5 * m * ((double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z);
+    r[1] += m * (phi - self);
+    r[2] += m * v.x;
+    r[3] += m * v.y;
+    r[4] += m * v.z;
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c)
+    for (int o = 16; o > 0; o >>= 1) r[c] += __shfl_down_sync(0xffffffffu, r[c], o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int c = 0; c < 5; ++c) s_r[warp][c] = r[c];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double v = 0.0;
+    for (int w = 0; w < kEThreads / 32; ++w) v += s_r[w][threadIdx.x];
+    epart[blockIdx.x * 5 + threadIdx.x] = v;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double t[5] = {0, 0, 0, 0, 0};
+    for (int b = 0; b < (int)gridDim.x; ++b)
+      for (int c = 0; c < 5; ++c) t[c] += __ldcg(&epart[b * 5 + c]);
+    double ke = t[0];
+    double pe = -0.5 * (double)G * t[1];
+    out[0] = ke + pe;
+    out[1] = ke;
+    out[2] = pe;
+    out[3] = t[2];
+    out[4] = t[3];
+    out[5] = t[4];
+    *ticket = 0u;
+  }
+}
+
+int launch_energy(Workspace& w, int n, const float4* pos, const float4* vel,
+                  float eps2, float G, cudaStream_t st) {
+  const int itiles = (n + kEThreads - 1) / kEThreads;
+  int js = (148 * 4 + itiles - 1) / itiles;
+  const int jt = (n + kETile - 1) / kETile;
+  if (js > jt) js = jt;
+  if (js < 1) js = 1;
+  int jchunk = (jt + js - 1) / js * kETile;
+  js = (n + jchunk - 1) / jchunk;
+  int rblocks = (n + kEThreads - 1) / kEThreads;
+  if (rblocks > 296) rblocks = 296;
+  NB_TRY(ws_reserve_energy(w, n, rblocks, js));
+  k_energy_phi<<<dim3(itiles, js), kEThreads, 0, st>>>(pos, n, eps2, jchunk,
+                                                        w.ephi);
+  NB_CUDA(cudaGetLastError());
+  k_energy_reduce<<<rblocks, kEThreads, 0, st>>>(
+      pos, vel, n, eps2, G, js, w.ephi, w.epart, w.eticket, w.eout);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+}  // namespace nb

@@ -1,0 +1,422 @@
+// LBVH build, rebuilt every step (src/forces_bh.cu:190-331):
+//   Morton keys (+ the radix sort's digit histograms, fused)
+//   onesweep LSD radix sort (+ the position gather, fused into the last pass)
+//   Karras radix-tree build
+//   bottom-up centres of mass / boxes / sizes, FP64 mass-weighted sums.
+#include "nb_internal.cuh"
+
+namespace nb {
+
+// ---------------------------------------------------------------------------
+// Morton keys.  Quantisation in IEEE round-to-nearest float32 with a
+// correctly rounded reciprocal, so the keys are bit-identical to the CPU
+// mirror (scripts/lbvh_check.py:45-54 on float32 input).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ uint64_t spread21(uint32_t x) {
+  uint64_t v = x & 0x1fffffu;
+  v = (v | (v << 32)) & 0x001f00000000ffffull;
+  v = (v | (v << 16)) & 0x001f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t quantise(float p, float lo, float inv,
+                                             float scale, float qmax) {
+  float t = __fmul_rn(__fsub_rn(p, lo), inv);
+  return (uint32_t)fminf(__fmul_rn(fmaxf(t, 0.f), scale), qmax);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ pos,
+                                                int n, const int* __restrict__ bbox,
+                                                K* keys, uint32_t* vals,
+                                                uint32_t* hist, int passes) {
+  __shared__ uint32_t s_hist[8 * kSortRadix];
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  const float lx = ord2f(bbox[0]), ly = ord2f(bbox[1]), lz = ord2f(bbox[2]);
+  const float hx = ord2f(bbox[3]), hy = ord2f(bbox[4]), hz = ord2f(bbox[5]);
+  const float ext =
+      fmaxf(__fsub_rn(hx, lx), fmaxf(__fsub_rn(hy, ly), __fsub_rn(hz, lz)));
+  const float inv = ext > 0.f ? __frcp_rn(ext) : 0.f;
+  const bool wide = sizeof(K) == 8;
+  const float scale = wide ? 2097152.f : 1024.f;
+  const float qmax = scale - 1.f;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+    float4 p = pos[i];
+    uint32_t qx = quantise(p.x, lx, inv, scale, qmax);
+    uint32_t qy = quantise(p.y, ly, inv, scale, qmax);
+    uint32_t qz = quantise(p.z, lz, inv, scale, qmax);
+    K k;
+    if (wide)
+      k = (K)((spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz));
+    else
+      k = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
+    keys[i] = k;
+    vals[i] = (uint32_t)i;
+    for (int ps = 0; ps < passes; ++ps)
+      atomicAdd(&s_hist[ps * kSortRadix + (uint32_t)((k >> (8 * ps)) & 0xffu)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) {
+    uint32_t c = s_hist[i];
+    if (c) atomicAdd(&hist[i], c);
+  }
+}
+
+int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  int passes = sort_passes(a.key_bits);
+  int blocks = (a.n + 255) / 256;
+  if (blocks > 2 * 148) blocks = 2 * 148;
+  if (a.key_bits == 63)
+    k_morton<uint64_t><<<blocks, 256, 0, st>>>(a.pos, a.n, w.bbox,
+                                               (uint64_t*)w.keys, w.vals, w.hist,
+                                               passes);
+  else
+    k_morton<uint32_t><<<blocks, 256, 0, st>>>(a.pos, a.n, w.bbox,
+                                               (uint32_t*)w.keys, w.vals, w.hist,
+                                               passes);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Onesweep LSD radix sort (Adinets & Merrill, 2022), 8-bit digits, stable.
+// Per pass one kernel: each CTA takes the next tile by ticket (so it only
+// waits on CTAs that are already running), ranks its keys with warp-level
+// match/popc, publishes its digit counts, resolves its global offsets by a
+// decoupled look-back over earlier tiles (bounded waits), and scatters.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1u;
+constexpr int kLookbackSpin = 1 << 20;
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <typename K, bool LAST>
+__global__ void __launch_bounds__(kSortThreads)
+    k_sort_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                K* __restrict__ kout, uint32_t* __restrict__ vout, int n,
+                int shift, const uint32_t* __restrict__ hist,
+                uint32_t* status, uint32_t* tile_ctr, unsigned* err,
+                const float4* __restrict__ pos, float4* __restrict__ pos_sorted) {
+  constexpr int W = kSortThreads / 32;
+  __shared__ uint32_t s_wc[W][kSortRadix];
+  __shared__ uint32_t s_base[kSortRadix];
+  __shared__ uint32_t s_scan[W];
+  __shared__ int s_tile;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
+  for (int i = tid; i < W * kSortRadix; i += kSortThreads) (&s_wc[0][0])[i] = 0u;
+
+  // global exclusive prefix of this pass's digit counts (one digit/thread)
+  const uint32_t h = hist[tid];
+  uint32_t incl = h;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_scan[warp] = incl;
+  __syncthreads();
+  uint32_t wofs = 0;
+  for (int i = 0; i < warp; ++i) wofs += s_scan[i];
+  const uint32_t gexcl = wofs + incl - h;
+
+  const int tile = s_tile;
+  const long seg = (long)tile * kSortTile + (long)warp * (kSortItems * 32);
+  K key[kSortItems];
+  uint32_t val[kSortItems];
+  uint32_t rank[kSortItems];
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    long idx = seg + k * 32 + lane;
+    bool ok = idx < n;
+    key[k] = ok ? kin[idx] : (K)0;
+    val[k] = ok ? vin[idx] : 0u;
+  }
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    long idx = seg + k * 32 + lane;
+    bool ok = idx < n;
+    uint32_t d = ok ? (uint32_t)((key[k] >> shift) & 0xffu) : 256u;
+    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t old = 0;
+    if (ok) {
+      old = s_wc[warp][d];
+      rank[k] = old + __popc(peers & lt);
+    }
+    __syncwarp();
+    if (ok && lane == __ffs(peers) - 1) s_wc[warp][d] = old + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // per digit: offsets of each warp inside the tile, and the tile's count
+  uint32_t run = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    uint32_t c = s_wc[w][tid];
+    s_wc[w][tid] = run;
+    run += c;
+  }
+  const uint32_t count = run;
+  uint32_t* my = status + (size_t)tile * kSortRadix + tid;
+  uint32_t excl = 0;
+  if (tile == 0) {
+    st_relaxed(my, kFlagInc | count);
+  } else {
+    st_relaxed(my, kFlagAgg | count);
+    for (int t = tile - 1; t >= 0; --t) {
+      const uint32_t* p = status + (size_t)t * kSortRadix + tid;
+      uint32_t s = ld_relaxed(p);
+      int spins = 0;
+      while ((s & ~kValMask) == 0u && spins < kLookbackSpin) {
+        if (spins > 64) __nanosleep(64);
+        s = ld_relaxed(p);
+        ++spins;
+      }
+      if ((s & ~kValMask) == 0u) {   // gave up: flag it and stop waiting
+        raise_err(err, NB_DEVERR_SORT);
+        break;
+      }
+      excl += s & kValMask;
+      if ((s & kFlagInc) != 0u) break;
+    }
+    st_relaxed(my, kFlagInc | ((excl + count) & kValMask));
+  }
+  s_base[tid] = gexcl + excl;
+  __syncthreads();
+
+#pragma unroll
+  for (int k = 0; k < kSortItems; ++k) {
+    long idx = seg + k * 32 + lane;
+    if (idx < n) {
+      uint32_t d = (uint32_t)((key[k] >> shift) & 0xffu);
+      uint32_t dst = s_base[d] + s_wc[warp][d] + rank[k];
+      if (dst < (uint32_t)n && val[k] < (uint32_t)n) {
+        kout[dst] = key[k];
+        vout[dst] = val[k];
+        if (LAST) pos_sorted[dst] = pos[val[k]];
+      } else {
+        raise_err(err, NB_DEVERR_SORT);
+      }
+    }
+  }
+}
+
+template <typename K>
+static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  const int passes = sort_passes(a.key_bits);
+  const int tiles = (a.n + kSortTile - 1) / kSortTile;
+  K* kin = (K*)w.keys;
+  K* kalt = (K*)w.keys_alt;
+  uint32_t* vin = w.vals;
+  uint32_t* valt = w.vals_alt;
+  for (int p = 0; p < passes; ++p) {
+    uint32_t* hist = w.hist + p * kSortRadix;
+    uint32_t* status = w.hist + 8 * kSortRadix + 8 + (size_t)p * w.status_tiles * kSortRadix;
+    uint32_t* ctr = w.tile_ctr + p;
+    if (p == passes - 1)
+      k_sort_pass<K, true><<<tiles, kSortThreads, 0, st>>>(
+          kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, a.pos,
+          w.pos_sorted);
+    else
+      k_sort_pass<K, false><<<tiles, kSortThreads, 0, st>>>(
+          kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, nullptr,
+          nullptr);
+    NB_CUDA(cudaGetLastError());
+    K* tk = kin; kin = kalt; kalt = tk;
+    uint32_t* tv = vin; vin = valt; valt = tv;
+  }
+  // after an even number of passes the result is back in keys / vals
+  if (kin != (K*)w.keys) {
+    void* t = w.keys; w.keys = w.keys_alt; w.keys_alt = t;
+    uint32_t* u = w.vals; w.vals = w.vals_alt; w.vals_alt = u;
+  }
+  return NB_OK;
+}
+
+int launch_sort(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  if (a.key_bits == 63) return sort_impl<uint64_t>(w, a, st);
+  return sort_impl<uint32_t>(w, a, st);
+}
+
+// ---------------------------------------------------------------------------
+// Karras 2012 radix tree over the sorted keys (src/forces_bh.cu:234-277).
+// delta(i, j): common-prefix length, -1 outside [0, n); equal keys continue
+// with the sorted index (word bits + clz(i ^ j)).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int clz_k(uint32_t x) { return __clz((int)x); }
+__device__ __forceinline__ int clz_k(uint64_t x) { return __clzll((long long)x); }
+
+template <typename K>
+__device__ __forceinline__ int delta_k(const K* __restrict__ keys, int n,
+                                       K ki, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  K x = ki ^ keys[j];
+  if (x) return clz_k(x);
+  return (int)(8 * sizeof(K)) + __clz(i ^ j);
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_karras(const K* __restrict__ keys,
+                                                int n, Node* nodes, int* parent,
+                                                int* visit) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) parent[0] = -1;
+  if (i >= n - 1) return;
+  const K ki = keys[i];
+  int d = (delta_k(keys, n, ki, i, i + 1) - delta_k(keys, n, ki, i, i - 1)) >= 0
+              ? 1 : -1;
+  int dmin = delta_k(keys, n, ki, i, i - d);
+  int lmax = 2;
+  while (delta_k(keys, n, ki, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t > 0; t >>= 1)
+    if (delta_k(keys, n, ki, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int first = min(i, j), last = max(i, j);
+  const K kf = keys[first];
+  int common = delta_k(keys, n, kf, first, last);
+  int split = first, step = last - first;
+  do {
+    step = (step + 1) >> 1;
+    if (split + step < last && delta_k(keys, n, kf, first, split + step) > common)
+      split += step;
+  } while (step > 1);
+  int left = (split == first) ? (n - 1 + split) : split;
+  int right = (split + 1 == last) ? (n - 1 + split + 1) : split + 1;
+  nodes[i].left = left;
+  nodes[i].right = right;
+  parent[left] = i;
+  parent[right] = i;
+  visit[i] = 0;
+}
+
+int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  int blocks = (a.n - 1 + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (a.key_bits == 63)
+    k_karras<uint64_t><<<blocks, 256, 0, st>>>((const uint64_t*)w.keys, a.n,
+                                               w.nodes, w.parent, w.visit);
+  else
+    k_karras<uint32_t><<<blocks, 256, 0, st>>>((const uint32_t*)w.keys, a.n,
+                                               w.nodes, w.parent, w.visit);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Bottom-up centres of mass (src/forces_bh.cu:281-331): every leaf climbs;
+// the first arrival at a node stops, the second combines both children
+// (left first, so the result does not depend on arrival order).  FP64
+// mass-weighted sums; node com = float(sum / mass); box = min/max of the
+// children's boxes; size2 = (longest edge)^2 in float.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int n,
+                                             Node* nodes,
+                                             const int* __restrict__ parent,
+                                             int* visit, double4* sums,
+                                             float4* box_lo, float4* box_hi,
+                                             unsigned* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int ni = n - 1;
+  int node = parent[ni + i];
+  // a valid tree is at most n-1 levels deep; the bound and the range checks
+  // only matter if an earlier phase failed (its error word is then set)
+  for (int guard = 0; node >= 0; ++guard) {
+    if (node >= ni || guard >= n) {
+      raise_err(err, NB_DEVERR_STACK);
+      return;
+    }
+    if (atomicAdd(&visit[node], 1) == 0) return;
+    __threadfence();
+    const int2 ch = __ldcg((const int2*)&nodes[node].left);
+    if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1) {
+      raise_err(err, NB_DEVERR_STACK);
+      return;
+    }
+    double s[2][4];
+    float l[2][3], h[2][3];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      int id = c == 0 ? ch.x : ch.y;
+      if (id >= ni) {
+        float4 p = ps[id - ni];
+        double m = (double)p.w;
+        s[c][0] = __dmul_rn((double)p.x, m);
+        s[c][1] = __dmul_rn((double)p.y, m);
+        s[c][2] = __dmul_rn((double)p.z, m);
+        s[c][3] = m;
+        l[c][0] = h[c][0] = p.x;
+        l[c][1] = h[c][1] = p.y;
+        l[c][2] = h[c][2] = p.z;
+      } else {
+        const double2* qp = reinterpret_cast<const double2*>(&sums[id]);
+        double2 q0 = __ldcg(qp), q1 = __ldcg(qp + 1);
+        float4 bl = __ldcg(&box_lo[id]);
+        float4 bh = __ldcg(&box_hi[id]);
+        s[c][0] = q0.x; s[c][1] = q0.y; s[c][2] = q1.x; s[c][3] = q1.y;
+        l[c][0] = bl.x; l[c][1] = bl.y; l[c][2] = bl.z;
+        h[c][0] = bh.x; h[c][1] = bh.y; h[c][2] = bh.z;
+      }
+    }
+    double4 q;
+    q.x = __dadd_rn(s[0][0], s[1][0]);
+    q.y = __dadd_rn(s[0][1], s[1][1]);
+    q.z = __dadd_rn(s[0][2], s[1][2]);
+    q.w = __dadd_rn(s[0][3], s[1][3]);
+    float4 com;
+    com.x = __double2float_rn(__ddiv_rn(q.x, q.w));
+    com.y = __double2float_rn(__ddiv_rn(q.y, q.w));
+    com.z = __double2float_rn(__ddiv_rn(q.z, q.w));
+    com.w = __double2float_rn(q.w);
+    float4 lo = make_float4(fminf(l[0][0], l[1][0]), fminf(l[0][1], l[1][1]),
+                            fminf(l[0][2], l[1][2]), 0.f);
+    float4 hi = make_float4(fmaxf(h[0][0], h[1][0]), fmaxf(h[0][1], h[1][1]),
+                            fmaxf(h[0][2], h[1][2]), 0.f);
+    float e = fmaxf(__fsub_rn(hi.x, lo.x),
+                    fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
+    sums[node] = q;
+    box_lo[node] = lo;
+    box_hi[node] = hi;
+    nodes[node].com = com;
+    nodes[node].size2 = __fmul_rn(e, e);
+    // publish before the parent's counter is touched
+    __threadfence();
+    node = parent[node];
+  }
+}
+
+int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  int blocks = (a.n + 255) / 256;
+  k_com<<<blocks, 256, 0, st>>>(w.pos_sorted, a.n, w.nodes, w.parent, w.visit,
+                                w.sums, w.box_lo, w.box_hi, w.err);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+}  // namespace nb

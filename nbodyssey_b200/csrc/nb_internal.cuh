@@ -1,0 +1,202 @@
+// Internal declarations shared by the kernel files and the C ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/nbody_b200.h"
+
+namespace nb {
+
+// ---------------------------------------------------------------------------
+// Error handling: every host entry point returns a status; the message for
+// the calling thread is kept in a thread-local string.
+// ---------------------------------------------------------------------------
+int set_error(int code, const std::string& msg);
+const char* last_error();
+
+#define NB_CUDA(call)                                                        \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess)                                                   \
+      return ::nb::set_error(NB_ERR_CUDA, std::string(#call) + ": " +        \
+                                              cudaGetErrorString(e_));       \
+  } while (0)
+
+#define NB_TRY(expr)            \
+  do {                          \
+    int rc_ = (expr);           \
+    if (rc_ != NB_OK) return rc_; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Layouts in HBM
+// ---------------------------------------------------------------------------
+// One internal LBVH node, 32 bytes: one sector per fetch in the walks.
+struct __align__(16) Node {
+  float4 com;     // centre of mass (x, y, z) and mass (w)
+  int left;       // child ids: internal [0, n-2], leaf i -> n-1+i
+  int right;
+  float size2;    // (longest edge of the node's tight box)^2
+  int pad;
+};
+
+// Walks keep their per-warp / per-thread stacks this deep.  A radix tree over
+// 63-bit keys with index tie-breaks is at most 63 + 31 levels deep and the
+// stack grows by at most one entry per level; an overflow raises
+// NB_DEVERR_STACK instead of writing past the stack.
+constexpr int kStack = 128;
+
+// Onesweep sort geometry.
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSortRadix = 256;
+
+// All-pairs source layout: particles are packed in pairs as two float4,
+// (x0, x1, y0, y1) and (z0, z1, m0, m1), padded with zero-mass particles to a
+// multiple of kSrcTile particles.
+constexpr int kSrcTile = 512;
+
+inline int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
+
+// Workspace: scratch of the force modules, grown only when n grows (the
+// reference's Scratch, src/forces_bh.cu:50-121).
+struct Workspace {
+  int cap = 0;          // particles
+  int key_bits = 0;     // layout the sort buffers were sized for
+  // tree
+  void* keys = nullptr;       // u32 or u64 [cap]
+  void* keys_alt = nullptr;
+  uint32_t* vals = nullptr;   // [cap]
+  uint32_t* vals_alt = nullptr;
+  float4* pos_sorted = nullptr;   // [cap]
+  Node* nodes = nullptr;          // [cap-1]
+  int* parent = nullptr;          // [2cap-1]
+  int* visit = nullptr;           // [cap-1]
+  double4* sums = nullptr;        // [cap-1] FP64 mass-weighted sums
+  float4* box_lo = nullptr;       // [cap-1]
+  float4* box_hi = nullptr;       // [cap-1]
+  // sort
+  uint32_t* hist = nullptr;       // [8][256] digit counts per pass
+  uint32_t* status = nullptr;     // [8][tiles][256] look-back words
+  uint32_t* tile_ctr = nullptr;   // [8] tile tickets
+  int status_tiles = 0;
+  // bounding box (ordered ints: lo xyz, hi xyz) + per-block partials
+  int* bbox = nullptr;            // [8]
+  int* bbox_part = nullptr;       // [kPrepMaxBlocks][6]
+  unsigned* bbox_ticket = nullptr;
+  // all-pairs
+  float4* src = nullptr;          // packed sources [2 * cap_pad/2]
+  int src_cap = 0;
+  float4* part = nullptr;         // j-split partials [jsplit][cap]
+  int part_cap = 0;               // elements
+  unsigned* tickets = nullptr;    // per i-tile tickets
+  int tickets_cap = 0;
+  // energy
+  double* epart = nullptr;        // per-block partials [blocks][6]
+  int epart_cap = 0;
+  double* ephi = nullptr;         // j-split phi partials [jsplit][cap]
+  int ephi_cap = 0;
+  double* eout = nullptr;         // [8]
+  unsigned* eticket = nullptr;    // last-block ticket of the energy reduce
+  double* h_eout = nullptr;       // pinned
+  // debug counters
+  int* counts = nullptr;          // [cap] interactions per sorted target
+  // error word
+  unsigned* err = nullptr;
+  unsigned* h_err = nullptr;      // pinned
+};
+
+constexpr int kPrepThreads = 256;
+constexpr int kPrepMaxBlocks = 1024;
+
+int ws_reserve(Workspace& w, int n, int key_bits);
+int ws_reserve_allpairs(Workspace& w, int n, int jsplit);
+int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit);
+void ws_free(Workspace& w);
+
+// ---------------------------------------------------------------------------
+// Launchers (kernel files).  All enqueue on `st`; none synchronise.
+// ---------------------------------------------------------------------------
+struct StepArgs {
+  int n;
+  float4* pos;      // hi (x, y, z, m), original order
+  float4* pos_lo;   // lo parts or nullptr (plain drift)
+  float4* vel;      // nullptr: no kick / drift
+  float4* acc;      // out: a(x), original order
+  float half_dt, dt;
+  float eps2, G, theta2;
+  int key_bits;
+  int traverse;
+  bool kick_drift;  // opening kick + drift before the force evaluation
+  bool kick_after;  // closing kick fused into the force epilogue
+  int* counts;      // debug: interactions per sorted target, or nullptr
+};
+
+// prep: [kick + drift] [+ bbox] [+ pack all-pairs sources] [+ zero sort scratch]
+int launch_prep(Workspace& w, const StepArgs& a, bool bbox, bool pack,
+                cudaStream_t st);
+int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st);
+int launch_sort(Workspace& w, const StepArgs& a, cudaStream_t st);
+int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st);
+int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st);
+int launch_walk(Workspace& w, const StepArgs& a, cudaStream_t st);
+int launch_allpairs(Workspace& w, const StepArgs& a, cudaStream_t st);
+// energy: {E, KE, PE, Px, Py, Pz} into w.eout (device); positions hi (+lo
+// for the kinetic part is not needed).
+int launch_energy(Workspace& w, int n, const float4* pos, const float4* vel,
+                  float eps2, float G, cudaStream_t st);
+int launch_flush(void* buf, size_t bytes, cudaStream_t st);
+int measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
+
+// all-pairs launch geometry (autotuned by n)
+struct APGeom {
+  int threads;   // per CTA
+  int k;         // targets per thread
+  int jsplit;    // CTAs along j per i-tile
+  int itiles;
+};
+APGeom allpairs_geometry(int n);
+
+// A view of a simulation handle's device state (defined in api.cu) for the
+// run loop in io.cu.
+struct SimView {
+  int n;
+  cudaStream_t stream;
+  float4* pos;
+  float4* vel;
+  Workspace* ws;
+  nb_params p;
+};
+}  // namespace nb
+struct nb_sim;
+namespace nb {
+int sim_view(nb_sim* s, SimView* v);
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int f2ord(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ord2f(int i) {
+  return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff);
+}
+
+__device__ __forceinline__ void raise_err(unsigned* err, unsigned bit) {
+  atomicOr(err, bit);
+}
+
+// rsqrt on the special-function unit (approximate, as the reference's
+// fast-math rsqrtf).
+__device__ __forceinline__ float mufu_rsqrt(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+}  // namespace nb
