@@ -77,7 +77,12 @@ def test_theta0_equals_allpairs(traverse):
     assert (cnt == n).all()
     exact = O.allpairs_f64(pos, EPS)
     r = rel_err(acc, exact)
-    assert np.median(r) < 2e-6 and np.percentile(r, 99) < 2e-5
+    # FP32 accumulation of n terms in tree order; the reference's own gate is
+    # a mean below 1e-4 (scripts/gpu_bench.sh:43; it published mean 1.7e-5,
+    # max 2.8e-4 at 20k, docs/PERFORMANCE.md:14-20).  Near-cancelling net
+    # forces set the tail.
+    assert r.mean() < 1e-4
+    assert np.median(r) < 1e-5 and np.percentile(r, 99) < 1e-3
 
 
 def test_compare_forces_gate():
