@@ -60,17 +60,25 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--force", choices=["bh", "naive"], default="bh",
+                    help="naive: time the all-pairs module instead (e.g. --n 262144)")
+    ap.add_argument("--walk", choices=["list", "dfs"], default="list",
+                    help="tree-walk kernel: batched list walk or depth-first walk")
     return ap.parse_args()
 
 
 def workload(args):
-    return {"workload": "Barnes-Hut %s walk, N=%d, theta %.2g, eps 0.05, dt 0.005, "
-                        "30-bit Morton keys, tree rebuilt every step" %
-                        (args.traverse, args.n, args.theta),
-            "n": args.n, "theta": args.theta, "traverse": args.traverse,
-            "key_bits": 30, "dt": 0.005, "eps": 0.05,
-            "l2": "flushed before every timed step (256 MB write)",
-            "parallelism": "replicas (one independent simulation per GPU)"}
+    common = {"n": args.n, "dt": 0.005, "eps": 0.05,
+              "l2": "flushed before every timed step (256 MB write)",
+              "parallelism": "replicas (one independent simulation per GPU)"}
+    if args.force == "naive":
+        return dict(common, workload="all-pairs, N=%d, eps 0.05, dt 0.005" % args.n,
+                    force="naive")
+    return dict(common, workload="Barnes-Hut %s walk, N=%d, theta %.2g, eps 0.05, "
+                                 "dt 0.005, 30-bit Morton keys, tree rebuilt every "
+                                 "step" % (args.traverse, args.n, args.theta),
+                theta=args.theta, traverse=args.traverse, key_bits=30, force="bh",
+                walk_kernel=args.walk)
 
 
 # --------------------------------------------------------------------------
@@ -122,14 +130,15 @@ class Clocks:
         self.proc = None
         self.path = None
 
-    def start(self):
-        fd, self.path = tempfile.mkstemp(prefix="nb_clocks_", suffix=".csv")
-        os.close(fd)
+    def start(self, append=False):
+        if not append or self.path is None:
+            fd, self.path = tempfile.mkstemp(prefix="nb_clocks_", suffix=".csv")
+            os.close(fd)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.index)],
-                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50", "-i", str(self.index)],
+                stdout=open(self.path, "a"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
@@ -146,7 +155,6 @@ class Clocks:
             f = [x.strip() for x in line.split(",")]
             if len(f) >= 9:
                 rows.append(f)
-        os.unlink(self.path)
         if not rows:
             return None
         def num(x):
@@ -245,8 +253,11 @@ def pinned_array(lib, shape, keep):
 
 
 def interactions(sim, api, params):
-    """Sum over particles of the per-thread-criterion interaction count."""
+    """Sum over particles of the per-thread-criterion interaction count
+    (all-pairs: n^2, the self term included as the reference counts it)."""
     from dataclasses import replace
+    if params.force == "naive":
+        return sim.n * sim.n
     sim.set_params(replace(params, traverse="thread"))
     _, cnt = sim.debug_forces()
     sim.set_params(params)
@@ -279,8 +290,9 @@ def run_b200(args, rank, world, local, pg):
     from nbodyssey_b200 import api, ic
     lib = L.load()
     L.check(lib.nb_set_device(local))
-    params = api.SimParams(dt=0.005, epsilon=0.05, theta=args.theta, force="bh",
-                           traverse=args.traverse, key_bits=30, compensated=True)
+    params = api.SimParams(dt=0.005, epsilon=0.05, theta=args.theta,
+                           force=args.force, traverse=args.traverse, key_bits=30,
+                           compensated=True, walk_kernel=args.walk)
     pos, vel = ic.bh_config(args.n, seed=rank)
     sim = api.Simulation(pos, vel, params)
     n = args.n
@@ -315,10 +327,12 @@ def run_b200(args, rank, world, local, pg):
     inter = 0.5 * (inter0 + inter1)
 
     # steady state through the captured graph, no flush (informational)
+    clocks.start(append=True)
     sim.record(0)
     sim.step(args.steps)
     sim.record(1)
     graph_ms = sim.elapsed_ms(0, 1)
+    clk = clocks.stop() or clk
 
     # end to end: pinned host state in, step, state out, every step
     keep = []
@@ -365,16 +379,18 @@ def run_b200(args, rank, world, local, pg):
         "graph_steps_per_s_no_flush": world * args.steps / (graph_ms * 1e-3),
         "phases_ms_per_step": {k: v / calls for k, v in phases.items() if v > 0},
         "interactions_per_particle": inter / n,
-        "gpu_launches": BH_KERNELS_PER_STEP * args.steps,
+        "gpu_launches": (BH_KERNELS_PER_STEP if args.force == "bh" else 2) * args.steps,
         "e2e": {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
                 "path": "nb_set_state_acc + nb_step + nb_get_{positions,"
                         "velocities,accelerations}, pinned host buffers, wall clock"},
-        "roofline": {"kernel": "k_walk_%s" % args.traverse, "bound": "fp32",
+        "roofline": {"kernel": (("k_walk_list" if args.walk == "list" else "k_walk_%s" % args.traverse) if args.force == "bh"
+                                else "k_allpairs"), "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic,
-                     "work": "20 flop x per-thread-criterion interactions "
-                             "(%.4g per step)" % inter,
+                     "work": ("20 flop x per-thread-criterion interactions "
+                              "(%.4g per step)" % inter if args.force == "bh" else
+                              "20 flop x N^2 pairs (%.4g per step)" % inter),
                      "peak_source": "measured on this GPU: FP32 FMA calibration "
                                     "kernel (scalar %.1f, packed f32x2 %.1f TFLOP/s)" %
                                     (ps.value, pp.value)},
@@ -388,7 +404,10 @@ def run_b200(args, rank, world, local, pg):
                            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
         "clocks": clk,
     }
-    if world == 1 and not args.no_cpu_baseline:
+    if args.force == "naive":
+        line.pop("roofline_build")
+        line.pop("interactions_per_particle")
+    if world == 1 and not args.no_cpu_baseline and args.force == "bh":
         line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
 

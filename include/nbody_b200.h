@@ -62,6 +62,9 @@ typedef struct nb_params {
                           63 (21 bits/axis, the reference's width) */
   int32_t compensated; /* 1: positions kept as a hi/lo float pair through the
                           drift (forces use hi); 0: plain float drift */
+  int32_t walk_kernel; /* 0: batched list walk (default); 1: depth-first walk,
+                          one node visit per step as the reference kernels.
+                          Both give the same interaction sets. */
 } nb_params;
 
 /* Fills the reference defaults: dt 0.01, eps 0.05, G 1, theta 0.5, naive,

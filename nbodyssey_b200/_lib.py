@@ -45,7 +45,8 @@ class nb_params(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_float), ("eps", ctypes.c_float),
                 ("G", ctypes.c_float), ("theta", ctypes.c_float),
                 ("force", ctypes.c_int32), ("traverse", ctypes.c_int32),
-                ("key_bits", ctypes.c_int32), ("compensated", ctypes.c_int32)]
+                ("key_bits", ctypes.c_int32), ("compensated", ctypes.c_int32),
+                ("walk_kernel", ctypes.c_int32)]
 
 
 class nb_run_stats(ctypes.Structure):

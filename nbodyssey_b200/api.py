@@ -42,6 +42,7 @@ class SimParams:
     traverse: str = BhTraversal.THREAD
     key_bits: int = 30
     compensated: bool = True
+    walk_kernel: str = "list"   # "list" (batched, default) or "dfs"
 
     def to_c(self):
         if self.force not in (ForceMethod.NAIVE, ForceMethod.BARNES_HUT):
@@ -57,6 +58,9 @@ class SimParams:
         p.traverse = L.NB_TRAVERSE_WARP if self.traverse == BhTraversal.WARP else L.NB_TRAVERSE_THREAD
         p.key_bits = int(self.key_bits)
         p.compensated = 1 if self.compensated else 0
+        if self.walk_kernel not in ("list", "dfs"):
+            raise ValueError("walk_kernel must be list or dfs")
+        p.walk_kernel = 0 if self.walk_kernel == "list" else 1
         return p
 
 

@@ -160,6 +160,8 @@ static int check_params(const nb_params* p) {
     return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
   if (p->key_bits != 30 && p->key_bits != 63)
     return set_error(NB_ERR_INVALID, "key_bits must be 30 or 63");
+  if (p->walk_kernel != 0 && p->walk_kernel != 1)
+    return set_error(NB_ERR_INVALID, "walk_kernel must be 0 or 1");
   return NB_OK;
 }
 
@@ -184,6 +186,7 @@ static StepArgs make_args(int n, float4* pos, float4* lo, float4* vel,
   a.theta2 = p.theta * p.theta;
   a.key_bits = p.key_bits;
   a.traverse = p.traverse;
+  a.walk_kernel = p.walk_kernel;
   a.kick_drift = false;
   a.kick_after = false;
   a.counts = nullptr;
@@ -436,6 +439,7 @@ void nb_params_default(nb_params* p) {
   p->traverse = NB_TRAVERSE_THREAD;
   p->key_bits = 30;
   p->compensated = 1;
+  p->walk_kernel = 0;
 }
 
 const char* nb_last_error(void) { return nb::last_error(); }
@@ -538,7 +542,8 @@ int nb_set_params(nb_sim* s, const nb_params* p) {
   bool changes_forces = p->force != s->p.force || p->eps != s->p.eps ||
                         p->G != s->p.G || p->theta != s->p.theta ||
                         p->traverse != s->p.traverse ||
-                        p->key_bits != s->p.key_bits;
+                        p->key_bits != s->p.key_bits ||
+                        p->walk_kernel != s->p.walk_kernel;
   if (p->compensated && !s->p.compensated)
     NB_CUDA(cudaMemsetAsync(s->pos_lo, 0, sizeof(float4) * s->n, s->stream));
   s->p = *p;

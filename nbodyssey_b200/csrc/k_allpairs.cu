@@ -13,35 +13,10 @@
 // * Small n splits the source range over `jsplit` CTAs per target tile; the
 //   last CTA of a tile (ticket) sums the partials in fixed order, so results
 //   are deterministic.  The leapfrog's closing kick is fused in the epilogue.
+#include "f32x2.cuh"
 #include "nb_internal.cuh"
 
 namespace nb {
-
-typedef unsigned long long f2;   // two packed floats
-
-__device__ __forceinline__ f2 pk2(float a, float b) {
-  f2 r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-  return r;
-}
-__device__ __forceinline__ void up2(f2 r, float& a, float& b) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
-}
-__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
-  f2 d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ f2 add2(f2 a, f2 b) {
-  f2 d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
-  f2 d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
 
 // --- mbarrier / bulk-copy helpers -----------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -1,0 +1,276 @@
+// Default Barnes-Hut walks (walk_kernel = 0): the reference's interaction
+// sets (src/forces_bh.cu:335-447), computed a warp-wide batch of nodes at a
+// time instead of one node per warp step.
+//
+// A warp owns 32 consecutive Morton-sorted targets.  It keeps a stack of
+// candidate nodes in shared memory and repeatedly takes up to 32 of them, one
+// per lane:
+//
+// * a leaf becomes an interaction-list entry;
+// * an internal node is decided against all targets at once.  A conservative
+//   test against the box of the 32 targets settles most nodes: if even the
+//   nearest point of the box accepts (size2 < theta2 * dmin2, with a 1e-5
+//   margin far above the 4e-7 rounding of the exact test), every target
+//   accepts; if even the farthest point rejects, every target rejects.  Only
+//   nodes in between run the exact per-target test (walk_common.cuh), so the
+//   decisions equal the per-target float tests bit for bit.
+//
+// Semantics:
+// * warp mode (traverse = warp, src/forces_bh.cu:395-447): a node opens when
+//   any live target rejects it; otherwise all targets take it;
+// * thread mode (traverse = thread, src/forces_bh.cu:335-377): each candidate
+//   carries the mask of targets whose own walk reaches it; targets that
+//   accept take it (entry with that mask), those that reject pass their mask
+//   to the children.  Every target gets exactly its per-thread interaction
+//   set.
+//
+// Accepted nodes and leaves go to a shared-memory interaction list (pairs of
+// entries interleaved as (x0,x1,y0,y1)(z0,z1,m0,m1)) that the lanes evaluate
+// for their own target with packed FP32 math, two entries per instruction.
+// Entries whose mask excludes a lane contribute with mass 0.
+//
+// If the candidate stack would overflow, the warp falls back to the
+// depth-first walk of the same semantics (same interaction set).
+#include "f32x2.cuh"
+#include "walk_common.cuh"
+
+namespace nb {
+
+constexpr int kLW = 4;          // warps per block
+constexpr int kCand = 1024;     // candidate stack entries per warp
+constexpr int kList = 64;       // interaction-list entries per warp
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <bool MASKED, bool COUNT>
+__global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
+  __shared__ float4 s_tgt[kLW][32];
+  __shared__ int s_cid[kLW][kCand];
+  __shared__ unsigned s_cmask[kLW][MASKED ? kCand : 1];
+  __shared__ __align__(16) float s_ent[kLW][kList * 4];
+  __shared__ unsigned s_emask[kLW][MASKED ? kList : 1];
+
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int wg = blockIdx.x * kLW + w;
+  const int n = a.n, ni = n - 1;
+  if (wg * 32 >= n) return;   // whole warp past the end
+  const int t = wg * 32 + lane;
+  const bool live = t < n;
+  const unsigned live_mask = __ballot_sync(full, live);
+  const unsigned lt = (1u << lane) - 1u;
+  // dead lanes (last warp only) copy particle n-1, a live lane of this warp,
+  // so the group box is the box of the live targets
+  const float4 bi = a.ps[live ? t : n - 1];
+  s_tgt[w][lane] = bi;
+  const float lox = warp_min(bi.x), loy = warp_min(bi.y), loz = warp_min(bi.z);
+  const float hix = warp_max(bi.x), hiy = warp_max(bi.y), hiz = warp_max(bi.z);
+  const float theta2 = a.theta2;
+
+  const f2 nx = pk2(-bi.x, -bi.x), ny = pk2(-bi.y, -bi.y), nz = pk2(-bi.z, -bi.z);
+  const f2 e2 = pk2(a.eps2, a.eps2);
+  f2 ax = 0ull, ay = 0ull, az = 0ull;
+  int cnt = 0;
+  float* ent = s_ent[w];
+
+  // evaluates list entries [0, lc) for this lane's target
+  auto flush = [&](int lc) {
+    if (lc & 1) {   // pad to a whole pair with a zero-mass entry
+      if (lane == 0) {
+        float* p = &ent[(lc >> 1) * 8 + 1];
+        p[0] = 0.f; p[2] = 0.f; p[4] = 0.f; p[6] = 0.f;
+        if (MASKED) s_emask[w][lc] = 0u;
+      }
+      __syncwarp();
+    }
+    const int np = (lc + 1) >> 1;
+    for (int q = 0; q < np; ++q) {
+      const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&ent[q * 8]);
+      const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&ent[q * 8 + 4]);
+      f2 m = B.y;
+      if (MASKED) {
+        const unsigned b0 = (s_emask[w][2 * q] >> lane) & 1u;
+        const unsigned b1 = (s_emask[w][2 * q + 1] >> lane) & 1u;
+        float m0, m1;
+        up2(B.y, m0, m1);
+        m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
+        if (COUNT) cnt += (int)(b0 + b1);
+      }
+      f2 dx = add2(A.x, nx);
+      f2 dy = add2(A.y, ny);
+      f2 dz = add2(B.x, nz);
+      f2 r2 = fma2(dz, dz, e2);
+      r2 = fma2(dy, dy, r2);
+      r2 = fma2(dx, dx, r2);
+      float r0, r1;
+      up2(r2, r0, r1);
+      f2 inv = pk2(mufu_rsqrt(r0), mufu_rsqrt(r1));
+      f2 wm = mul2(inv, m);
+      f2 i2 = mul2(inv, inv);
+      f2 f = mul2(wm, i2);
+      ax = fma2(dx, f, ax);
+      ay = fma2(dy, f, ay);
+      az = fma2(dz, f, az);
+    }
+    if (!MASKED && COUNT) cnt += lc;
+    __syncwarp();
+  };
+
+  int sp = 1, lc = 0;
+  if (lane == 0) {
+    s_cid[w][0] = 0;   // root
+    if (MASKED) s_cmask[w][0] = live_mask;
+  }
+  __syncwarp();
+  bool overflow = false;
+  for (int guard = 0; sp > 0; ++guard) {
+    if (sp + 32 > kCand || guard > 2 * n) {   // uniform across the warp
+      overflow = true;
+      break;
+    }
+    const int take = min(sp, 32);
+    const int base = sp - take;
+    const bool has = lane < take;
+    int id = 0;
+    unsigned M = live_mask;
+    if (has) {
+      id = s_cid[w][base + lane];
+      if (MASKED) M = s_cmask[w][base + lane];
+    }
+    __syncwarp();
+    sp = base;
+
+    bool want_ent = false, want_push = false;
+    float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+    unsigned emask = 0u, pmask = 0u;
+    int cl = 0, cr = 0;
+    if (has && id >= ni) {
+      e = a.ps[id - ni];
+      want_ent = true;
+      emask = M;
+    } else if (has) {
+      const Node nd = a.nodes[id];
+      const float cx = nd.com.x, cy = nd.com.y, cz = nd.com.z;
+      const float ex = fmaxf(fmaxf(lox - cx, cx - hix), 0.f);
+      const float ey = fmaxf(fmaxf(loy - cy, cy - hiy), 0.f);
+      const float ez = fmaxf(fmaxf(loz - cz, cz - hiz), 0.f);
+      const float dmin2 = ex * ex + ey * ey + ez * ez;
+      const float fx = fmaxf(fabsf(cx - lox), fabsf(cx - hix));
+      const float fy = fmaxf(fabsf(cy - loy), fabsf(cy - hiy));
+      const float fz = fmaxf(fabsf(cz - loz), fabsf(cz - hiz));
+      const float dmax2 = fx * fx + fy * fy + fz * fz;
+      unsigned accm;
+      if (nd.size2 < theta2 * dmin2 * 0.99999f) {
+        accm = M;
+      } else if (nd.size2 > theta2 * dmax2 * 1.00001f) {
+        accm = 0u;
+      } else {
+        accm = 0u;
+        unsigned rem = M;
+        while (rem) {
+          const int k = __ffs(rem) - 1;
+          rem &= rem - 1u;
+          const float4 q = s_tgt[w][k];
+          if (accepts(nd.size2, theta2, cx, cy, cz, q.x, q.y, q.z)) {
+            accm |= 1u << k;
+          } else if (!MASKED) {
+            break;   // one rejection opens the node for the whole warp
+          }
+        }
+        if (!MASKED && rem != 0u) accm = 0u;
+      }
+      if (MASKED) {
+        if (accm) {
+          want_ent = true;
+          e = nd.com;
+          emask = accm;
+        }
+        const unsigned om = M & ~accm;
+        if (om) {
+          want_push = true;
+          cl = nd.left;
+          cr = nd.right;
+          pmask = om;
+        }
+      } else if (accm == M) {
+        want_ent = true;
+        e = nd.com;
+      } else {
+        want_push = true;
+        cl = nd.left;
+        cr = nd.right;
+      }
+    }
+    const unsigned eb = __ballot_sync(full, want_ent);
+    if (want_ent) {
+      const int k = lc + __popc(eb & lt);
+      float* p = &ent[(k >> 1) * 8 + (k & 1)];
+      p[0] = e.x; p[2] = e.y; p[4] = e.z; p[6] = e.w;
+      if (MASKED) s_emask[w][k] = emask;
+    }
+    lc += __popc(eb);
+    const unsigned pb = __ballot_sync(full, want_push);
+    if (want_push) {
+      const int k = sp + 2 * __popc(pb & lt);
+      s_cid[w][k] = cl;
+      s_cid[w][k + 1] = cr;
+      if (MASKED) {
+        s_cmask[w][k] = pmask;
+        s_cmask[w][k + 1] = pmask;
+      }
+    }
+    sp += 2 * __popc(pb);
+    __syncwarp();
+    if (lc >= 32) {
+      flush(lc);
+      lc = 0;
+    }
+  }
+
+  float3 ai;
+  if (!overflow) {
+    if (lc) flush(lc);
+    float u, v;
+    up2(ax, u, v); ai.x = u + v;
+    up2(ay, u, v); ai.y = u + v;
+    up2(az, u, v); ai.z = u + v;
+  } else {
+    // same interaction set by the depth-first walk; the candidate stack's
+    // shared memory serves as the warp stack
+    cnt = 0;
+    __syncwarp();
+    if (MASKED)
+      ai = dfs_walk_thread<COUNT>(a, bi, &cnt);
+    else
+      ai = dfs_walk_warp<COUNT>(a, bi, live, s_cid[w], &cnt);
+  }
+  if (live) {
+    epilogue(a, t, ai);
+    if (COUNT) a.counts[t] = cnt;
+  }
+}
+
+int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st) {
+  const int warps = (a.n + 31) / 32;
+  const int blocks = (warps + kLW - 1) / kLW;
+  if (masked) {
+    if (a.counts) k_walk_list<true, true><<<blocks, kLW * 32, 0, st>>>(a);
+    else k_walk_list<true, false><<<blocks, kLW * 32, 0, st>>>(a);
+  } else {
+    if (a.counts) k_walk_list<false, true><<<blocks, kLW * 32, 0, st>>>(a);
+    else k_walk_list<false, false><<<blocks, kLW * 32, 0, st>>>(a);
+  }
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+}  // namespace nb

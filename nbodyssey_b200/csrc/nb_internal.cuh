@@ -131,6 +131,7 @@ struct StepArgs {
   float eps2, G, theta2;
   int key_bits;
   int traverse;
+  int walk_kernel;  // 0 list walk, 1 depth-first walk
   bool kick_drift;  // opening kick + drift before the force evaluation
   bool kick_after;  // closing kick fused into the force epilogue
   int* counts;      // debug: interactions per sorted target, or nullptr

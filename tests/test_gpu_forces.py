@@ -25,39 +25,42 @@ def rel_err(a, b):
     return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
 
 
-def bh_forces(pos, theta, traverse, bits=30, eps=EPS):
+def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="list"):
     prm = api.SimParams(epsilon=eps, theta=theta, force="bh", traverse=traverse,
-                        key_bits=bits)
+                        key_bits=bits, walk_kernel=walk)
     with api.Simulation(pos, np.zeros_like(pos), prm) as sim:
         acc, cnt = sim.debug_forces()
     return acc[:, :3].astype(np.float64), cnt.astype(np.int64)
 
 
+@pytest.mark.parametrize("walk", ["list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 @pytest.mark.parametrize("theta", [0.3, 0.5, 0.7])
-@pytest.mark.parametrize("n", [1000, 20_000])
-def test_walk_matches_oracle(n, theta, traverse):
+@pytest.mark.parametrize("n", [1000, 20_000, 20_001])
+def test_walk_matches_oracle(n, theta, traverse, walk):
     pos, _ = ic.two_disks(n, seed=11)
-    acc, cnt = bh_forces(pos, theta, traverse)
+    acc, cnt = bh_forces(pos, theta, traverse, walk=walk)
     ref, inter = O.Tree(pos, 30).forces(theta, EPS, traverse=traverse)
     assert np.array_equal(cnt, inter)
     assert rel_err(acc, ref).max() < 2e-5
 
 
+@pytest.mark.parametrize("walk", ["list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
-def test_walk_matches_oracle_63bit(traverse):
+def test_walk_matches_oracle_63bit(traverse, walk):
     pos, _ = ic.two_disks(30_000, seed=12)
-    acc, cnt = bh_forces(pos, 0.5, traverse, bits=63)
+    acc, cnt = bh_forces(pos, 0.5, traverse, bits=63, walk=walk)
     ref, inter = O.Tree(pos, 63).forces(0.5, EPS, traverse=traverse)
     assert np.array_equal(cnt, inter)
     assert rel_err(acc, ref).max() < 2e-5
 
 
-def test_walk_1m_subsample():
+@pytest.mark.parametrize("walk", ["list", "dfs"])
+def test_walk_1m_subsample(walk):
     """1M particles, theta 0.5 warp walk: counts of every target equal the
     oracle's (which walks only 4096 sampled warps)."""
     pos, _ = ic.bh_config(1_000_000, seed=5)
-    acc, cnt = bh_forces(pos, 0.5, "warp")
+    acc, cnt = bh_forces(pos, 0.5, "warp", walk=walk)
     tree = O.Tree(pos, 30)
     rng = np.random.default_rng(0)
     warps = np.sort(rng.choice((1_000_000 + 31) // 32, 4096, replace=False))
@@ -69,11 +72,12 @@ def test_walk_1m_subsample():
     assert rel_err(acc[orig], ref_w[live]).max() < 2e-5
 
 
+@pytest.mark.parametrize("walk", ["list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
-def test_theta0_equals_allpairs(traverse):
+def test_theta0_equals_allpairs(traverse, walk):
     n = 20_000
     pos, _ = ic.two_disks(n, seed=13)
-    acc, cnt = bh_forces(pos, 0.0, traverse)
+    acc, cnt = bh_forces(pos, 0.0, traverse, walk=walk)
     assert (cnt == n).all()
     exact = O.allpairs_f64(pos, EPS)
     r = rel_err(acc, exact)
@@ -160,3 +164,30 @@ def test_determinism():
         b1 = sim.compute_forces()
         b2 = sim.compute_forces()
     assert np.array_equal(b1, b2)
+
+
+@pytest.mark.parametrize("traverse", ["thread", "warp"])
+def test_list_walk_duplicates_and_clumps(traverse):
+    """Coincident clumps (zero-size nodes, duplicate keys) through the list
+    walk's box prefilter: interaction sets still equal the oracle's."""
+    rng = np.random.default_rng(9)
+    p = np.zeros((6000, 4), np.float32)
+    p[:, :3] = rng.normal(size=(6000, 3)).astype(np.float32)
+    p[:1500, :3] = np.float32([0.25, -0.5, 0.75])
+    p[1500:1800, :3] = p[1600, :3]
+    p[:, 3] = 1.0 / 6000
+    for theta in (0.0, 0.5, 1.0):
+        acc, cnt = bh_forces(p, theta, traverse)
+        ref, inter = O.Tree(p, 30).forces(theta, EPS, traverse=traverse)
+        assert np.array_equal(cnt, inter)
+        assert rel_err(acc, ref).max() < 2e-5
+
+
+def test_list_and_dfs_thread_walks_agree():
+    """The lane-masked list walk gives every target its per-thread
+    interaction set: counts equal the one-thread-per-target walk's."""
+    pos, _ = ic.two_disks(50_000, seed=17)
+    a1, c1 = bh_forces(pos, 0.5, "thread", walk="list")
+    a2, c2 = bh_forces(pos, 0.5, "thread", walk="dfs")
+    assert np.array_equal(c1, c2)
+    assert rel_err(a1, a2.astype(np.float64)).max() < 2e-5
