@@ -1,7 +1,7 @@
 """GPU parity of the force modules.
 
 * Barnes-Hut walks: the interaction set of every target equals the oracle's
-  (counts bit-exact, thread and warp walks); forces within 2e-5 relative of
+  (counts bit-exact, thread and warp walks); forces within 5e-5 relative of
   the oracle's FP64 sum over the same set (FP32 pair math with an
   approximate rsqrt accumulates ~1e-6).
 * theta = 0 reproduces all-pairs: every target touches n leaves; forces within
@@ -25,6 +25,14 @@ def rel_err(a, b):
     return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
 
 
+def assert_walk_close(acc, ref):
+    """Same interaction set, FP32 sum (approximate rsqrt, ~10^3 terms in the
+    walk's order) against the FP64 sum: median < 1e-6, max < 5e-5."""
+    r = rel_err(acc, ref)
+    assert np.median(r) < 1e-6
+    assert r.max() < 5e-5
+
+
 def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="list"):
     prm = api.SimParams(epsilon=eps, theta=theta, force="bh", traverse=traverse,
                         key_bits=bits, walk_kernel=walk)
@@ -42,7 +50,7 @@ def test_walk_matches_oracle(n, theta, traverse, walk):
     acc, cnt = bh_forces(pos, theta, traverse, walk=walk)
     ref, inter = O.Tree(pos, 30).forces(theta, EPS, traverse=traverse)
     assert np.array_equal(cnt, inter)
-    assert rel_err(acc, ref).max() < 2e-5
+    assert_walk_close(acc, ref)
 
 
 @pytest.mark.parametrize("walk", ["list", "dfs"])
@@ -52,7 +60,7 @@ def test_walk_matches_oracle_63bit(traverse, walk):
     acc, cnt = bh_forces(pos, 0.5, traverse, bits=63, walk=walk)
     ref, inter = O.Tree(pos, 63).forces(0.5, EPS, traverse=traverse)
     assert np.array_equal(cnt, inter)
-    assert rel_err(acc, ref).max() < 2e-5
+    assert_walk_close(acc, ref)
 
 
 @pytest.mark.parametrize("walk", ["list", "dfs"])
@@ -69,7 +77,7 @@ def test_walk_1m_subsample(walk):
     live = sorted_idx < 1_000_000
     orig = tree.perm.astype(np.int64)[sorted_idx[live]]
     assert np.array_equal(cnt[orig], np.repeat(inter_w, 32)[live])
-    assert rel_err(acc[orig], ref_w[live]).max() < 2e-5
+    assert_walk_close(acc[orig], ref_w[live])
 
 
 @pytest.mark.parametrize("walk", ["list", "dfs"])
@@ -180,7 +188,7 @@ def test_list_walk_duplicates_and_clumps(traverse):
         acc, cnt = bh_forces(p, theta, traverse)
         ref, inter = O.Tree(p, 30).forces(theta, EPS, traverse=traverse)
         assert np.array_equal(cnt, inter)
-        assert rel_err(acc, ref).max() < 2e-5
+        assert_walk_close(acc, ref)
 
 
 def test_list_and_dfs_thread_walks_agree():
@@ -190,4 +198,4 @@ def test_list_and_dfs_thread_walks_agree():
     a1, c1 = bh_forces(pos, 0.5, "thread", walk="list")
     a2, c2 = bh_forces(pos, 0.5, "thread", walk="dfs")
     assert np.array_equal(c1, c2)
-    assert rel_err(a1, a2.astype(np.float64)).max() < 2e-5
+    assert_walk_close(a1, a2.astype(np.float64))
