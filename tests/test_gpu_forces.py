@@ -188,7 +188,11 @@ def test_list_walk_duplicates_and_clumps(traverse):
         acc, cnt = bh_forces(p, theta, traverse)
         ref, inter = O.Tree(p, 30).forces(theta, EPS, traverse=traverse)
         assert np.array_equal(cnt, inter)
-        assert_walk_close(acc, ref)
+        if theta == 0.0:   # all 6000 terms: the theta = 0 band
+            r = rel_err(acc, ref)
+            assert r.mean() < 1e-4 and np.median(r) < 1e-5
+        else:
+            assert_walk_close(acc, ref)
 
 
 def test_list_and_dfs_thread_walks_agree():
