@@ -3,6 +3,8 @@
 //   onesweep LSD radix sort (+ the position gather, fused into the last pass)
 //   Karras radix-tree build
 //   bottom-up centres of mass / boxes / sizes, FP64 mass-weighted sums.
+#include <cuda/atomic>
+
 #include "nb_internal.cuh"
 
 namespace nb {
@@ -352,8 +354,10 @@ __global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int 
       raise_err(err, NB_DEVERR_STACK);
       return;
     }
-    if (atomicAdd(&visit[node], 1) == 0) return;
-    __threadfence();
+    // acq_rel: releases this thread's writes of the child it finished and
+    // acquires the sibling's, which the other arrival released
+    cuda::atomic_ref<int, cuda::thread_scope_device> arrivals(visit[node]);
+    if (arrivals.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
     const int2 ch = __ldcg((const int2*)&nodes[node].left);
     if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1) {
       raise_err(err, NB_DEVERR_STACK);
@@ -405,8 +409,7 @@ __global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int 
     box_hi[node] = hi;
     nodes[node].com = com;
     nodes[node].size2 = __fmul_rn(e, e);
-    // publish before the parent's counter is touched
-    __threadfence();
+    // published by the release half of the next level's fetch_add
     node = parent[node];
   }
 }

@@ -53,7 +53,6 @@ __device__ __forceinline__ float warp_max(float v) {
 
 template <bool MASKED, bool COUNT>
 __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
-  __shared__ float4 s_tgt[kLW][32];
   __shared__ int s_cid[kLW][kCand];
   __shared__ unsigned s_cmask[kLW][MASKED ? kCand : 1];
   __shared__ __align__(16) float s_ent[kLW][kList * 4];
@@ -71,7 +70,6 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
   // dead lanes (last warp only) copy particle n-1, a live lane of this warp,
   // so the group box is the box of the live targets
   const float4 bi = a.ps[live ? t : n - 1];
-  s_tgt[w][lane] = bi;
   const float lox = warp_min(bi.x), loy = warp_min(bi.y), loz = warp_min(bi.z);
   const float hix = warp_max(bi.x), hiy = warp_max(bi.y), hiz = warp_max(bi.z);
   const float theta2 = a.theta2;
@@ -151,15 +149,22 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
 
     bool want_ent = false, want_push = false;
     float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-    unsigned emask = 0u, pmask = 0u;
+    unsigned emask = 0u, pmask = 0u, accm = 0u;
     int cl = 0, cr = 0;
+    float s2 = 0.f;
+    bool amb = false;
+    const bool is_int = has && id < ni;
     if (has && id >= ni) {
       e = a.ps[id - ni];
       want_ent = true;
       emask = M;
-    } else if (has) {
+    } else if (is_int) {
       const Node nd = a.nodes[id];
-      const float cx = nd.com.x, cy = nd.com.y, cz = nd.com.z;
+      e = nd.com;
+      cl = nd.left;
+      cr = nd.right;
+      s2 = nd.size2;
+      const float cx = e.x, cy = e.y, cz = e.z;
       const float ex = fmaxf(fmaxf(lox - cx, cx - hix), 0.f);
       const float ey = fmaxf(fmaxf(loy - cy, cy - hiy), 0.f);
       const float ez = fmaxf(fmaxf(loz - cz, cz - hiz), 0.f);
@@ -168,46 +173,39 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       const float fy = fmaxf(fabsf(cy - loy), fabsf(cy - hiy));
       const float fz = fmaxf(fabsf(cz - loz), fabsf(cz - hiz));
       const float dmax2 = fx * fx + fy * fy + fz * fz;
-      unsigned accm;
-      if (nd.size2 < theta2 * dmin2 * 0.99999f) {
-        accm = M;
-      } else if (nd.size2 > theta2 * dmax2 * 1.00001f) {
-        accm = 0u;
-      } else {
-        accm = 0u;
-        unsigned rem = M;
-        while (rem) {
-          const int k = __ffs(rem) - 1;
-          rem &= rem - 1u;
-          const float4 q = s_tgt[w][k];
-          if (accepts(nd.size2, theta2, cx, cy, cz, q.x, q.y, q.z)) {
-            accm |= 1u << k;
-          } else if (!MASKED) {
-            break;   // one rejection opens the node for the whole warp
-          }
-        }
-        if (!MASKED && rem != 0u) accm = 0u;
-      }
+      if (s2 < theta2 * dmin2 * 0.99999f) accm = M;
+      else if (s2 > theta2 * dmax2 * 1.00001f) accm = 0u;
+      else amb = true;
+    }
+    // nodes the box cannot settle: every lane tests its own target against
+    // each of them in turn (node broadcast by shuffle, one ballot per node)
+    unsigned ambb = __ballot_sync(full, amb);
+    while (ambb) {
+      const int src = __ffs(ambb) - 1;
+      ambb &= ambb - 1u;
+      const float sx = __shfl_sync(full, e.x, src);
+      const float sy = __shfl_sync(full, e.y, src);
+      const float sz = __shfl_sync(full, e.z, src);
+      const float ss = __shfl_sync(full, s2, src);
+      const bool ok = !live || accepts(ss, theta2, sx, sy, sz, bi.x, bi.y, bi.z);
+      const unsigned b = __ballot_sync(full, ok);
+      if (lane == src) accm = b & M;
+    }
+    if (is_int) {
       if (MASKED) {
         if (accm) {
           want_ent = true;
-          e = nd.com;
           emask = accm;
         }
         const unsigned om = M & ~accm;
         if (om) {
           want_push = true;
-          cl = nd.left;
-          cr = nd.right;
           pmask = om;
         }
       } else if (accm == M) {
         want_ent = true;
-        e = nd.com;
       } else {
         want_push = true;
-        cl = nd.left;
-        cr = nd.right;
       }
     }
     const unsigned eb = __ballot_sync(full, want_ent);
