@@ -57,6 +57,8 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
   __shared__ unsigned s_cmask[kLW][MASKED ? kCand : 1];
   __shared__ __align__(16) float s_ent[kLW][kList * 4];
   __shared__ unsigned s_emask[kLW][MASKED ? kList : 1];
+  __shared__ __align__(16) float s_amb[kLW][32 * 4];   // ambiguous nodes, pairs
+  __shared__ unsigned s_res[kLW][32];                  // their accept ballots
 
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -177,19 +179,43 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       else if (s2 > theta2 * dmax2 * 1.00001f) accm = 0u;
       else amb = true;
     }
-    // nodes the box cannot settle: every lane tests its own target against
-    // each of them in turn (node broadcast by shuffle, one ballot per node)
-    unsigned ambb = __ballot_sync(full, amb);
-    while (ambb) {
-      const int src = __ffs(ambb) - 1;
-      ambb &= ambb - 1u;
-      const float sx = __shfl_sync(full, e.x, src);
-      const float sy = __shfl_sync(full, e.y, src);
-      const float sz = __shfl_sync(full, e.z, src);
-      const float ss = __shfl_sync(full, s2, src);
-      const bool ok = !live || accepts(ss, theta2, sx, sy, sz, bi.x, bi.y, bi.z);
-      const unsigned b = __ballot_sync(full, ok);
-      if (lane == src) accm = b & M;
+    // nodes the box cannot settle: their owners stage them in shared memory
+    // (pairs interleaved as (cx0,cx1,cy0,cy1)(cz0,cz1,s0,s1)); every lane
+    // tests its own target against two of them per packed instruction, in
+    // the float order of accepts(), and one ballot per node is written back
+    const unsigned ambb = __ballot_sync(full, amb);
+    if (ambb) {
+      const int na = __popc(ambb);
+      const int ka = __popc(ambb & lt);
+      if (amb) {
+        float* p = &s_amb[w][(ka >> 1) * 8 + (ka & 1)];
+        p[0] = e.x; p[2] = e.y; p[4] = e.z; p[6] = s2;
+      }
+      if (na & 1) {   // pad: a node every target accepts (size2 = -1)
+        if (lane == 0) {
+          float* p = &s_amb[w][(na >> 1) * 8 + 1];
+          p[0] = 0.f; p[2] = 0.f; p[4] = 0.f; p[6] = -1.f;
+        }
+      }
+      __syncwarp();
+      const f2 th2 = pk2(theta2, theta2);
+      for (int q = 0; q < (na + 1) >> 1; ++q) {
+        const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&s_amb[w][q * 8]);
+        const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&s_amb[w][q * 8 + 4]);
+        const f2 dx = add2(A.x, nx), dy = add2(A.y, ny), dz = add2(B.x, nz);
+        const f2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+        float t0, t1, z0, z1;
+        up2(mul2(th2, d2), t0, t1);
+        up2(B.y, z0, z1);
+        const unsigned b0 = __ballot_sync(full, !live || z0 < t0);
+        const unsigned b1 = __ballot_sync(full, !live || z1 < t1);
+        if (lane == 0) {
+          s_res[w][2 * q] = b0;
+          s_res[w][2 * q + 1] = b1;
+        }
+      }
+      __syncwarp();
+      if (amb) accm = s_res[w][ka] & M;
     }
     if (is_int) {
       if (MASKED) {
