@@ -193,6 +193,18 @@ NB_API int nb_compute_forces_dev(nb_workspace* w, int n, const float* d_pos4,
  * (no low-order state); d_acc must hold a(x) on entry, a(x_new) on exit. */
 NB_API int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_vel4,
                          float* d_acc4, const nb_params* p, void* stream);
+/* No counterpart in the reference.  All-pairs accelerations (the same as
+ * nb_compute_forces_dev with NB_FORCE_NAIVE) for callers that cannot
+ * allocate device memory: the scratch lives in a fixed file-scope device
+ * array (about 4.6 MB per GPU, held until exit), so the call allocates
+ * nothing.  n must be <= 32768 (NB_ERR_INVALID otherwise).  The first call on
+ * each device looks up the array's device address; make that first call
+ * before any stream capture.  Calls share the array: calls whose GPU work
+ * overlaps race and must be serialised by the caller.  Asynchronous on
+ * `stream`. */
+NB_API int nb_compute_forces_naive_static(int n, const float* d_pos4,
+                                          float* d_acc4, float eps, float G,
+                                          void* stream);
 /* total_energy(sys, p) (src/integrator.cuh:21): synchronous, e3 on host. */
 NB_API int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,
                         const float* d_vel4, const nb_params* p, double* e3,

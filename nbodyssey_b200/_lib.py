@@ -106,6 +106,7 @@ SIGNATURES = {
     "nb_compute_forces_dev": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_leapfrog_step_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_total_energy_dev": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _P, _P]),
+    "nb_compute_forces_naive_static": (_I, [_I, _P, _P, _F, _F, _P]),
     "nb_read_ic": (_I, [_S, ctypes.POINTER(_I), _P, _P]),
     "nb_write_ic": (_I, [_S, _I, _P, _P]),
     "nb_write_frame": (_I, [_S, _I, _I, _P]),

@@ -13,6 +13,10 @@
 // * Small n splits the source range over `jsplit` CTAs per target tile; the
 //   last CTA of a tile (ticket) sums the partials in fixed order, so results
 //   are deterministic.  The leapfrog's closing kick is fused in the epilogue.
+#include <cmath>
+#include <mutex>
+#include <string>
+
 #include "f32x2.cuh"
 #include "nb_internal.cuh"
 
@@ -358,4 +362,121 @@ int launch_energy(Workspace& w, int n, const float4* pos, const float4* vel,
   return NB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// All-pairs forces with no allocation at all (nb_compute_forces_naive_static).
+//
+// Some callers cannot allocate device memory when they need forces: a host
+// application that owns every device allocation itself (a fixed memory
+// budget reserved at start-up, an allocator that is closed after
+// initialisation, a plugin that must not grow the process's footprint).
+// Such a caller hands over its particle and acceleration buffers and gets
+// the same all-pairs accelerations as nb_compute_forces_dev with
+// NB_FORCE_NAIVE, computed by the same kernel, but with the scratch it needs
+// (packed sources, per-chunk partial sums, tile tickets) taken from the
+// file-scope device array below instead of from a workspace.
+//
+// The array is sized for kStaticMaxN particles and at most kStaticMaxSplit
+// source chunks per target tile: about 4.6 MB, held on every GPU that loads
+// the library until the process exits.  Every call shares it and it keeps
+// the previous call's contents; the tickets, the only part that must start at
+// zero, are cleared at the start of each call.  Calls whose GPU work overlaps
+// (different streams, or different host threads on one device) race on the
+// array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+constexpr int kStaticMaxN = 32768;
+constexpr int kStaticMaxSplit = 8;
+constexpr size_t kStaticSrcBytes = (size_t)kStaticMaxN * sizeof(float4);
+constexpr size_t kStaticPartBytes = (size_t)kStaticMaxSplit * kStaticMaxN * sizeof(float4);
+constexpr size_t kStaticTailBytes = 256;   // tickets (<= 33 words) + error word
+static __device__ __align__(256) unsigned char
+    g_static_scratch[kStaticSrcBytes + kStaticPartBytes + kStaticTailBytes];
+
+// Packs positions into the pair-interleaved source layout (zero-mass pad).
+__global__ void k_pack_static(const float4* __restrict__ pos, int n, int npairs,
+                              float4* __restrict__ src) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npairs;
+       q += gridDim.x * blockDim.x) {
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 a = 2 * q < n ? pos[2 * q] : z;
+    const float4 b = 2 * q + 1 < n ? pos[2 * q + 1] : z;
+    src[2 * q] = make_float4(a.x, b.x, a.y, b.y);
+    src[2 * q + 1] = make_float4(a.z, b.z, a.w, b.w);
+  }
+}
+
+// Device address of g_static_scratch for the current device.  Host code may
+// not pass the symbol itself (in host code it names a host-side stand-in), so
+// the address is looked up once per device with that device current.
+static int static_scratch_address(unsigned char** out) {
+  static std::mutex mu;
+  static unsigned char* addr[64] = {};
+  int dev = 0;
+  NB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(NB_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess)
+      return set_error(NB_ERR_CUDA, std::string("cudaGetSymbolAddress(g_static_scratch): ") +
+                                        cudaGetErrorString(e));
+    addr[dev] = (unsigned char*)p;
+  }
+  *out = addr[dev];
+  return NB_OK;
+}
+
 }  // namespace nb
+
+extern "C" int nb_compute_forces_naive_static(int n, const float* d_pos4,
+                                              float* d_acc4, float eps, float G,
+                                              void* stream) {
+  using namespace nb;
+  if (!d_pos4 || !d_acc4) return set_error(NB_ERR_INVALID, "NULL device pointer");
+  if (n <= 0) return set_error(NB_ERR_INVALID, "n must be > 0");
+  if (n > kStaticMaxN)
+    return set_error(NB_ERR_INVALID,
+                     "n = " + std::to_string(n) + " exceeds the " +
+                         std::to_string(kStaticMaxN) +
+                         "-particle limit of nb_compute_forces_naive_static's "
+                         "fixed scratch; use nb_compute_forces_dev");
+  if (!(eps > 0.f) || !std::isfinite(eps) || !std::isfinite(G))
+    return set_error(NB_ERR_INVALID, "eps must be a finite value > 0 and G finite");
+  unsigned char* base = nullptr;
+  NB_TRY(static_scratch_address(&base));
+  cudaStream_t st = (cudaStream_t)stream;
+  float4* src = (float4*)base;
+  float4* part = (float4*)(base + kStaticSrcBytes);
+  unsigned* tail = (unsigned*)(base + kStaticSrcBytes + kStaticPartBytes);
+  NB_CUDA(cudaMemsetAsync(tail, 0, kStaticTailBytes, st));
+
+  APGeom g = allpairs_geometry(n);
+  const int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
+  const int jtiles = npad / kSrcTile;
+  int js = g.jsplit < kStaticMaxSplit ? g.jsplit : kStaticMaxSplit;
+  const int jt_per = (jtiles + js - 1) / js;
+  js = (jtiles + jt_per - 1) / jt_per;
+
+  const int npairs = npad / 2;
+  k_pack_static<<<(npairs + 255) / 256, 256, 0, st>>>((const float4*)d_pos4, n,
+                                                      npairs, src);
+  NB_CUDA(cudaGetLastError());
+  APArgs a;
+  a.n = n;
+  a.pos = (const float4*)d_pos4;
+  a.src = src;
+  a.npad = npad;
+  a.jsplit = js;
+  a.jchunk = jt_per * kSrcTile;
+  a.eps2 = eps * eps;
+  a.G = G;
+  a.half_dt = 0.f;
+  a.acc = (float4*)d_acc4;
+  a.vel = nullptr;
+  a.part = part;
+  a.tickets = tail;
+  a.err = tail + 48;
+  k_allpairs<256, 4><<<dim3(g.itiles, js), 256, 0, st>>>(a);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
