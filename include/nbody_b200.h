@@ -211,6 +211,33 @@ NB_API int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,
                         void* stream);
 
 /* ======================================================================
+ * Ensembles: many independent simulations advanced together, one set of
+ * launches per step for all of them (captured as one CUDA graph).  No
+ * reference counterpart (the reference runs one simulation per process);
+ * each simulation's results are bit-identical to running it alone through
+ * the handle API with the same parameters.  Barnes-Hut, 30-bit keys.
+ * ==================================================================== */
+typedef struct nb_ensemble nb_ensemble;
+/* n[nsims] particle counts; pos4 / vel4 hold all simulations' rows back to
+ * back (sum of n rows); params[nsims], one per simulation (dt, eps, G, theta,
+ * traverse, compensated may differ).  nsims <= 1023. */
+NB_API int nb_ensemble_create(int nsims, const int* n, const float* pos4,
+                              const float* vel4, const nb_params* params,
+                              nb_ensemble** out);
+NB_API int nb_ensemble_destroy(nb_ensemble* e);
+NB_API int nb_ensemble_size(const nb_ensemble* e, int* nsims, long long* particles);
+/* nsteps leapfrog steps of every simulation (a(x0) first, once). */
+NB_API int nb_ensemble_step(nb_ensemble* e, int nsteps);
+NB_API int nb_ensemble_sync(nb_ensemble* e);
+NB_API int nb_ensemble_set_graphs(nb_ensemble* e, int enable);
+NB_API int nb_ensemble_get_state(nb_ensemble* e, int sim, float* pos4, float* vel4);
+NB_API int nb_ensemble_get_accelerations(nb_ensemble* e, int sim, float* acc4);
+/* e3[nsims][3] = {E, KE, PE} of every simulation, FP64 reductions. */
+NB_API int nb_ensemble_energy(nb_ensemble* e, double* e3);
+NB_API int nb_ensemble_record(nb_ensemble* e, int slot /* 0..15 */);
+NB_API int nb_ensemble_elapsed_ms(nb_ensemble* e, int slot0, int slot1, double* ms);
+
+/* ======================================================================
  * Files and the run loop (src/main.cu:115-215, docs/FORMATS.md).
  * ==================================================================== */
 /* load_ic (src/main.cu:115-128).  Call with pos4 = vel4 = NULL to get n. */

@@ -107,6 +107,17 @@ SIGNATURES = {
     "nb_leapfrog_step_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_total_energy_dev": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _P, _P]),
     "nb_compute_forces_naive_static": (_I, [_I, _P, _P, _F, _F, _P]),
+    "nb_ensemble_create": (_I, [_I, _P, _P, _P, _P, _PP]),
+    "nb_ensemble_destroy": (_I, [_P]),
+    "nb_ensemble_size": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong)]),
+    "nb_ensemble_step": (_I, [_P, _I]),
+    "nb_ensemble_sync": (_I, [_P]),
+    "nb_ensemble_set_graphs": (_I, [_P, _I]),
+    "nb_ensemble_get_state": (_I, [_P, _I, _P, _P]),
+    "nb_ensemble_get_accelerations": (_I, [_P, _I, _P]),
+    "nb_ensemble_energy": (_I, [_P, _P]),
+    "nb_ensemble_record": (_I, [_P, _I]),
+    "nb_ensemble_elapsed_ms": (_I, [_P, _I, _I, ctypes.POINTER(_D)]),
     "nb_read_ic": (_I, [_S, ctypes.POINTER(_I), _P, _P]),
     "nb_write_ic": (_I, [_S, _I, _P, _P]),
     "nb_write_frame": (_I, [_S, _I, _I, _P]),

@@ -115,13 +115,21 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-template <typename K, bool LAST>
+// pass modes: a middle pass; the last pass (also gathers the sorted
+// positions); the last pass of an ensemble sort (also remaps each
+// simulation's keys into its slot range)
+constexpr int kSortMid = 0;
+constexpr int kSortLast = 1;
+constexpr int kSortLastEnsemble = 2;
+
+template <typename K, int MODE>
 __global__ void __launch_bounds__(kSortThreads)
     k_sort_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                 K* __restrict__ kout, uint32_t* __restrict__ vout, int n,
                 int shift, const uint32_t* __restrict__ hist,
                 uint32_t* status, uint32_t* tile_ctr, unsigned* err,
-                const float4* __restrict__ pos, float4* __restrict__ pos_sorted) {
+                const float4* __restrict__ pos, float4* __restrict__ pos_sorted,
+                const SimDesc* __restrict__ sims, int nsims) {
   constexpr int W = kSortThreads / 32;
   __shared__ uint32_t s_wc[W][kSortRadix];
   __shared__ uint32_t s_base[kSortRadix];
@@ -218,9 +226,20 @@ __global__ void __launch_bounds__(kSortThreads)
       uint32_t d = (uint32_t)((key[k] >> shift) & 0xffu);
       uint32_t dst = s_base[d] + s_wc[warp][d] + rank[k];
       if (dst < (uint32_t)n && val[k] < (uint32_t)n) {
+        if (MODE == kSortLastEnsemble) {
+          // keys arrive grouped by simulation (id in bits 30+); rank d within
+          // the group goes to slot base + (d - coff); unused slots drop out
+          const uint32_t s = (uint32_t)(key[k] >> 30);
+          if (s >= (uint32_t)nsims) continue;
+          dst = (uint32_t)sims[s].base + (dst - (uint32_t)sims[s].coff);
+          if (dst >= (uint32_t)n) {
+            raise_err(err, NB_DEVERR_SORT);
+            continue;
+          }
+        }
         kout[dst] = key[k];
         vout[dst] = val[k];
-        if (LAST) pos_sorted[dst] = pos[val[k]];
+        if (MODE != kSortMid) pos_sorted[dst] = pos[val[k]];
       } else {
         raise_err(err, NB_DEVERR_SORT);
       }
@@ -241,13 +260,13 @@ static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
     uint32_t* status = w.hist + 8 * kSortRadix + 8 + (size_t)p * w.status_tiles * kSortRadix;
     uint32_t* ctr = w.tile_ctr + p;
     if (p == passes - 1)
-      k_sort_pass<K, true><<<tiles, kSortThreads, 0, st>>>(
+      k_sort_pass<K, kSortLast><<<tiles, kSortThreads, 0, st>>>(
           kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, a.pos,
-          w.pos_sorted);
+          w.pos_sorted, nullptr, 0);
     else
-      k_sort_pass<K, false><<<tiles, kSortThreads, 0, st>>>(
+      k_sort_pass<K, kSortMid><<<tiles, kSortThreads, 0, st>>>(
           kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, nullptr,
-          nullptr);
+          nullptr, nullptr, 0);
     NB_CUDA(cudaGetLastError());
     K* tk = kin; kin = kalt; kalt = tk;
     uint32_t* tv = vin; vin = valt; valt = tv;
@@ -282,11 +301,11 @@ __device__ __forceinline__ int delta_k(const K* __restrict__ keys, int n,
   return (int)(8 * sizeof(K)) + __clz(i ^ j);
 }
 
+// Internal node i of the tree over keys[0, n) (indices local to the tree).
 template <typename K>
-__global__ void __launch_bounds__(256) k_karras(const K* __restrict__ keys,
-                                                int n, Node* nodes, int* parent,
-                                                int* visit) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void karras_node(const K* __restrict__ keys, int n,
+                                            int i, Node* nodes, int* parent,
+                                            int* visit) {
   if (i == 0) parent[0] = -1;
   if (i >= n - 1) return;
   const K ki = keys[i];
@@ -317,6 +336,14 @@ __global__ void __launch_bounds__(256) k_karras(const K* __restrict__ keys,
   visit[i] = 0;
 }
 
+template <typename K>
+__global__ void __launch_bounds__(256) k_karras(const K* __restrict__ keys,
+                                                int n, Node* nodes, int* parent,
+                                                int* visit) {
+  karras_node<K>(keys, n, blockIdx.x * blockDim.x + threadIdx.x, nodes, parent,
+                 visit);
+}
+
 int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
   int blocks = (a.n - 1 + 255) / 256;
   if (blocks < 1) blocks = 1;
@@ -337,13 +364,13 @@ int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
 // mass-weighted sums; node com = float(sum / mass); box = min/max of the
 // children's boxes; size2 = (longest edge)^2 in float.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int n,
-                                             Node* nodes,
-                                             const int* __restrict__ parent,
-                                             int* visit, double4* sums,
-                                             float4* box_lo, float4* box_hi,
-                                             unsigned* err) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// The climb from leaf i of the tree over ps[0, n) (indices local to the tree).
+__device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
+                                          int i, Node* nodes,
+                                          const int* __restrict__ parent,
+                                          int* visit, double4* sums,
+                                          float4* box_lo, float4* box_hi,
+                                          unsigned* err) {
   if (i >= n) return;
   const int ni = n - 1;
   int node = parent[ni + i];
@@ -414,10 +441,146 @@ __global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int 
   }
 }
 
+__global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int n,
+                                             Node* nodes,
+                                             const int* __restrict__ parent,
+                                             int* visit, double4* sums,
+                                             float4* box_lo, float4* box_hi,
+                                             unsigned* err) {
+  com_climb(ps, n, blockIdx.x * blockDim.x + threadIdx.x, nodes, parent, visit,
+            sums, box_lo, box_hi, err);
+}
+
 int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st) {
   int blocks = (a.n + 255) / 256;
   k_com<<<blocks, 256, 0, st>>>(w.pos_sorted, a.n, w.nodes, w.parent, w.visit,
                                 w.sums, w.box_lo, w.box_hi, w.err);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ensemble tree build.  One global sort of keys (sim << 30) | morton30 groups
+// the simulations (stable, so each group keeps its own Morton order); its
+// last pass scatters group s into slots [base_s, base_s + n_s).  Karras and
+// the centre-of-mass climb then run per simulation on local indices, so each
+// tree is the one the simulation alone would build (the 64-bit keys shift
+// every delta by 32, which keeps the order of the deltas).
+// ---------------------------------------------------------------------------
+constexpr uint64_t kEnsDeadKey = ((uint64_t)kEnsMaxSims << 30) | 0x3fffffffull;
+
+__global__ void __launch_bounds__(256) k_ens_morton(EnsArgs e) {
+  constexpr int P = (kEnsKeyBits + 7) / 8;
+  __shared__ uint32_t s_hist[P * kSortRadix];
+  for (int i = threadIdx.x; i < P * kSortRadix; i += blockDim.x) s_hist[i] = 0;
+  __syncthreads();
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < e.nslots;
+       slot += gridDim.x * blockDim.x) {
+    uint64_t key = kEnsDeadKey;
+    const int s = e.blk_sim[slot >> 5];
+    if (s >= 0) {
+      const SimDesc d = e.sims[s];
+      const int local = slot - d.base;
+      if (d.active && local < d.n) {
+        const float lx = ord2f(e.bbox_min[4 * s]), ly = ord2f(e.bbox_min[4 * s + 1]),
+                    lz = ord2f(e.bbox_min[4 * s + 2]);
+        const float hx = ord2f(e.bbox_max[4 * s]), hy = ord2f(e.bbox_max[4 * s + 1]),
+                    hz = ord2f(e.bbox_max[4 * s + 2]);
+        const float ext =
+            fmaxf(__fsub_rn(hx, lx), fmaxf(__fsub_rn(hy, ly), __fsub_rn(hz, lz)));
+        const float inv = ext > 0.f ? __frcp_rn(ext) : 0.f;
+        const float4 p = e.pos[slot];
+        const uint32_t m = (spread10(quantise(p.x, lx, inv, 1024.f, 1023.f)) << 2) |
+                           (spread10(quantise(p.y, ly, inv, 1024.f, 1023.f)) << 1) |
+                           spread10(quantise(p.z, lz, inv, 1024.f, 1023.f));
+        key = ((uint64_t)s << 30) | m;
+      }
+    }
+    e.keys[slot] = key;
+    e.perm[slot] = (uint32_t)slot;
+#pragma unroll
+    for (int ps = 0; ps < P; ++ps)
+      atomicAdd(&s_hist[ps * kSortRadix + (uint32_t)((key >> (8 * ps)) & 0xffu)], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < P * kSortRadix; i += blockDim.x) {
+    const uint32_t c = s_hist[i];
+    if (c) atomicAdd(&e.hist[i], c);
+  }
+}
+
+int launch_ens_morton(const EnsArgs& e, cudaStream_t st) {
+  int blocks = (e.nslots + 255) / 256;
+  if (blocks > 4 * 148) blocks = 4 * 148;
+  k_ens_morton<<<blocks, 256, 0, st>>>(e);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// Sorts; on return e.keys / e.perm point at the buffers holding the result.
+int launch_ens_sort(EnsArgs& e, cudaStream_t st) {
+  const int passes = (kEnsKeyBits + 7) / 8;
+  const int tiles = (e.nslots + kSortTile - 1) / kSortTile;
+  uint64_t* kin = e.keys;
+  uint64_t* kalt = e.keys_alt;
+  uint32_t* vin = e.perm;
+  uint32_t* valt = e.perm_alt;
+  for (int p = 0; p < passes; ++p) {
+    uint32_t* hist = e.hist + p * kSortRadix;
+    uint32_t* status = e.status + (size_t)p * e.status_tiles * kSortRadix;
+    uint32_t* ctr = e.tile_ctr + p;
+    if (p == passes - 1)
+      k_sort_pass<uint64_t, kSortLastEnsemble><<<tiles, kSortThreads, 0, st>>>(
+          kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err, e.pos,
+          e.pos_sorted, e.sims, e.nsims);
+    else
+      k_sort_pass<uint64_t, kSortMid><<<tiles, kSortThreads, 0, st>>>(
+          kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err, nullptr,
+          nullptr, nullptr, 0);
+    NB_CUDA(cudaGetLastError());
+    uint64_t* tk = kin; kin = kalt; kalt = tk;
+    uint32_t* tv = vin; vin = valt; valt = tv;
+  }
+  e.keys = kin;
+  e.keys_alt = kalt;
+  e.perm = vin;
+  e.perm_alt = valt;
+  return NB_OK;
+}
+
+__global__ void __launch_bounds__(256) k_ens_karras(EnsArgs e) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= e.nslots) return;
+  const int s = e.blk_sim[g >> 5];
+  if (s < 0) return;
+  const SimDesc d = e.sims[s];
+  if (!d.active || d.n < 2) return;
+  karras_node<uint64_t>(e.keys + d.base, d.n, g - d.base, e.nodes + d.base,
+                        e.parent + 2 * d.base, e.visit + d.base);
+}
+
+__global__ void __launch_bounds__(256) k_ens_com(EnsArgs e) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= e.nslots) return;
+  const int s = e.blk_sim[g >> 5];
+  if (s < 0) return;
+  const SimDesc d = e.sims[s];
+  if (!d.active || d.n < 2) return;
+  com_climb(e.pos_sorted + d.base, d.n, g - d.base, e.nodes + d.base,
+            e.parent + 2 * d.base, e.visit + d.base, e.sums + d.base,
+            e.box_lo + d.base, e.box_hi + d.base, e.err);
+}
+
+int launch_ens_build(const EnsArgs& e, cudaStream_t st) {
+  const int blocks = (e.nslots + 255) / 256;
+  k_ens_karras<<<blocks, 256, 0, st>>>(e);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+int launch_ens_com(const EnsArgs& e, cudaStream_t st) {
+  const int blocks = (e.nslots + 255) / 256;
+  k_ens_com<<<blocks, 256, 0, st>>>(e);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }

@@ -174,6 +174,82 @@ int launch_prep(Workspace& w, const StepArgs& s, bool bbox, bool pack,
   return NB_OK;
 }
 
+// Ensemble prep: kick + drift of every live slot, each simulation's bounding
+// box (warp min/max, then one atomic per component and warp; warps never mix
+// simulations), and zeroing of the sort scratch.  The boxes must hold the
+// empty sentinels on entry (launch_ens_prep sets them).
+template <bool KD>
+__global__ void __launch_bounds__(kPrepThreads) k_ens_prep(EnsArgs e,
+                                                           uint32_t* zero,
+                                                           int zero_words) {
+  const int stride = gridDim.x * blockDim.x;   // a multiple of 32
+  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < e.nslots;
+       slot += stride) {
+    const int s = e.blk_sim[slot >> 5];         // the same for the whole warp
+    if (s < 0) continue;
+    const SimDesc d = e.sims[s];
+    const bool valid = d.active && slot - d.base < d.n;
+    int r[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000,
+                (int)0x80000000, (int)0x80000000};
+    if (valid) {
+      float4 x = e.pos[slot];
+      if (KD) {
+        float4 v = e.vel[slot];
+        const float4 ac = e.acc[slot];
+        v.x = __fmaf_rn(d.half_dt, ac.x, v.x);
+        v.y = __fmaf_rn(d.half_dt, ac.y, v.y);
+        v.z = __fmaf_rn(d.half_dt, ac.z, v.z);
+        e.vel[slot] = v;
+        if (d.compensated) {
+          float4 l = e.pos_lo[slot];
+          drift_comp(x.x, l.x, v.x, d.dt);
+          drift_comp(x.y, l.y, v.y, d.dt);
+          drift_comp(x.z, l.z, v.z, d.dt);
+          e.pos_lo[slot] = l;
+        } else {
+          x.x = __fmaf_rn(d.dt, v.x, x.x);
+          x.y = __fmaf_rn(d.dt, v.y, x.y);
+          x.z = __fmaf_rn(d.dt, v.z, x.z);
+        }
+        e.pos[slot] = x;
+      }
+      r[0] = r[3] = f2ord(x.x);
+      r[1] = r[4] = f2ord(x.y);
+      r[2] = r[5] = f2ord(x.z);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r[c] = __reduce_min_sync(0xffffffffu, r[c]);
+      r[c + 3] = __reduce_max_sync(0xffffffffu, r[c + 3]);
+    }
+    if ((threadIdx.x & 31) == 0 && d.active) {
+      for (int c = 0; c < 3; ++c) {
+        atomicMin(&e.bbox_min[4 * s + c], r[c]);
+        atomicMax(&e.bbox_max[4 * s + c], r[c + 3]);
+      }
+    }
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < zero_words; i += stride)
+    zero[i] = 0u;
+}
+
+int launch_ens_prep(const EnsArgs& e, cudaStream_t st) {
+  // empty boxes: 0x7f7f7f7f (a large positive ordered value) for the minima,
+  // 0x80808080 (a large negative one) for the maxima
+  NB_CUDA(cudaMemsetAsync(e.bbox_min, 0x7f, sizeof(int) * 4 * e.nsims, st));
+  NB_CUDA(cudaMemsetAsync(e.bbox_max, 0x80, sizeof(int) * 4 * e.nsims, st));
+  const int zero_words = 8 * kSortRadix + 8 + 8 * e.status_tiles * kSortRadix;
+  int blocks = (e.nslots + kPrepThreads - 1) / kPrepThreads;
+  if (blocks > 4 * 148) blocks = 4 * 148;
+  if (blocks < 1) blocks = 1;
+  if (e.kick_drift)
+    k_ens_prep<true><<<blocks, kPrepThreads, 0, st>>>(e, e.hist, zero_words);
+  else
+    k_ens_prep<false><<<blocks, kPrepThreads, 0, st>>>(e, e.hist, zero_words);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
 // L2 flush used by the benchmark between timed steps: writes a buffer larger
 // than the 126 MB L2.
 __global__ void k_flush(uint4* buf, size_t n) {

@@ -55,6 +55,7 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
   a.acc = s.acc;
   a.vel = s.kick_after ? s.vel : nullptr;
   a.counts = s.counts;
+  a.perm_limit = s.n;
   a.err = w.err;
   if (s.walk_kernel == 0)
     return launch_walk_list(a, s.traverse == NB_TRAVERSE_THREAD, st);

@@ -51,18 +51,25 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
-template <bool MASKED, bool COUNT>
-__global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
-  __shared__ int s_cid[kLW][kCand];
-  __shared__ unsigned s_cmask[kLW][MASKED ? kCand : 1];
-  __shared__ __align__(16) float s_ent[kLW][kList * 4];
-  __shared__ unsigned s_emask[kLW][MASKED ? kList : 1];
-  __shared__ __align__(16) float s_amb[kLW][32 * 4];   // ambiguous nodes, pairs
-  __shared__ unsigned s_res[kLW][32];                  // their accept ballots
+// Shared memory of one block: per warp a candidate stack (+ lane masks), the
+// interaction list (+ masks), the staged ambiguous nodes and their ballots.
+template <bool MASKED>
+struct ListSmem {
+  int cid[kLW][kCand];
+  unsigned cmask[kLW][MASKED ? kCand : 1];
+  __align__(16) float ent[kLW][kList * 4];
+  unsigned emask[kLW][MASKED ? kList : 1];
+  __align__(16) float amb[kLW][32 * 4];   // ambiguous nodes, pairs
+  unsigned res[kLW][32];                  // their accept ballots
+};
 
+// The walk of warp `wg` (targets 32wg .. 32wg+31 of the tree in `a`); all
+// 32 lanes of the warp call it.
+template <bool MASKED, bool COUNT>
+__device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
+                                               ListSmem<MASKED>& sm) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int wg = blockIdx.x * kLW + w;
   const int n = a.n, ni = n - 1;
   if (wg * 32 >= n) return;   // whole warp past the end
   const int t = wg * 32 + lane;
@@ -80,7 +87,7 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
   const f2 e2 = pk2(a.eps2, a.eps2);
   f2 ax = 0ull, ay = 0ull, az = 0ull;
   int cnt = 0;
-  float* ent = s_ent[w];
+  float* ent = sm.ent[w];
 
   // evaluates list entries [0, lc) for this lane's target
   auto flush = [&](int lc) {
@@ -88,7 +95,7 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       if (lane == 0) {
         float* p = &ent[(lc >> 1) * 8 + 1];
         p[0] = 0.f; p[2] = 0.f; p[4] = 0.f; p[6] = 0.f;
-        if (MASKED) s_emask[w][lc] = 0u;
+        if (MASKED) sm.emask[w][lc] = 0u;
       }
       __syncwarp();
     }
@@ -98,8 +105,8 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&ent[q * 8 + 4]);
       f2 m = B.y;
       if (MASKED) {
-        const unsigned b0 = (s_emask[w][2 * q] >> lane) & 1u;
-        const unsigned b1 = (s_emask[w][2 * q + 1] >> lane) & 1u;
+        const unsigned b0 = (sm.emask[w][2 * q] >> lane) & 1u;
+        const unsigned b1 = (sm.emask[w][2 * q + 1] >> lane) & 1u;
         float m0, m1;
         up2(B.y, m0, m1);
         m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
@@ -127,8 +134,8 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
 
   int sp = 1, lc = 0;
   if (lane == 0) {
-    s_cid[w][0] = 0;   // root
-    if (MASKED) s_cmask[w][0] = live_mask;
+    sm.cid[w][0] = 0;   // root
+    if (MASKED) sm.cmask[w][0] = live_mask;
   }
   __syncwarp();
   bool overflow = false;
@@ -143,8 +150,8 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
     int id = 0;
     unsigned M = live_mask;
     if (has) {
-      id = s_cid[w][base + lane];
-      if (MASKED) M = s_cmask[w][base + lane];
+      id = sm.cid[w][base + lane];
+      if (MASKED) M = sm.cmask[w][base + lane];
     }
     __syncwarp();
     sp = base;
@@ -188,20 +195,20 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       const int na = __popc(ambb);
       const int ka = __popc(ambb & lt);
       if (amb) {
-        float* p = &s_amb[w][(ka >> 1) * 8 + (ka & 1)];
+        float* p = &sm.amb[w][(ka >> 1) * 8 + (ka & 1)];
         p[0] = e.x; p[2] = e.y; p[4] = e.z; p[6] = s2;
       }
       if (na & 1) {   // pad: a node every target accepts (size2 = -1)
         if (lane == 0) {
-          float* p = &s_amb[w][(na >> 1) * 8 + 1];
+          float* p = &sm.amb[w][(na >> 1) * 8 + 1];
           p[0] = 0.f; p[2] = 0.f; p[4] = 0.f; p[6] = -1.f;
         }
       }
       __syncwarp();
       const f2 th2 = pk2(theta2, theta2);
       for (int q = 0; q < (na + 1) >> 1; ++q) {
-        const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&s_amb[w][q * 8]);
-        const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&s_amb[w][q * 8 + 4]);
+        const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&sm.amb[w][q * 8]);
+        const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&sm.amb[w][q * 8 + 4]);
         const f2 dx = add2(A.x, nx), dy = add2(A.y, ny), dz = add2(B.x, nz);
         const f2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
         float t0, t1, z0, z1;
@@ -210,12 +217,12 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
         const unsigned b0 = __ballot_sync(full, !live || z0 < t0);
         const unsigned b1 = __ballot_sync(full, !live || z1 < t1);
         if (lane == 0) {
-          s_res[w][2 * q] = b0;
-          s_res[w][2 * q + 1] = b1;
+          sm.res[w][2 * q] = b0;
+          sm.res[w][2 * q + 1] = b1;
         }
       }
       __syncwarp();
-      if (amb) accm = s_res[w][ka] & M;
+      if (amb) accm = sm.res[w][ka] & M;
     }
     if (is_int) {
       if (MASKED) {
@@ -239,17 +246,17 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
       const int k = lc + __popc(eb & lt);
       float* p = &ent[(k >> 1) * 8 + (k & 1)];
       p[0] = e.x; p[2] = e.y; p[4] = e.z; p[6] = e.w;
-      if (MASKED) s_emask[w][k] = emask;
+      if (MASKED) sm.emask[w][k] = emask;
     }
     lc += __popc(eb);
     const unsigned pb = __ballot_sync(full, want_push);
     if (want_push) {
       const int k = sp + 2 * __popc(pb & lt);
-      s_cid[w][k] = cl;
-      s_cid[w][k + 1] = cr;
+      sm.cid[w][k] = cl;
+      sm.cid[w][k + 1] = cr;
       if (MASKED) {
-        s_cmask[w][k] = pmask;
-        s_cmask[w][k + 1] = pmask;
+        sm.cmask[w][k] = pmask;
+        sm.cmask[w][k + 1] = pmask;
       }
     }
     sp += 2 * __popc(pb);
@@ -275,12 +282,57 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
     if (MASKED)
       ai = dfs_walk_thread<COUNT>(a, bi, &cnt);
     else
-      ai = dfs_walk_warp<COUNT>(a, bi, live, s_cid[w], &cnt);
+      ai = dfs_walk_warp<COUNT>(a, bi, live, sm.cid[w], &cnt);
   }
   if (live) {
     epilogue(a, t, ai);
     if (COUNT) a.counts[t] = cnt;
   }
+}
+
+template <bool MASKED, bool COUNT>
+__global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
+  __shared__ ListSmem<MASKED> sm;
+  walk_list_warp<MASKED, COUNT>(a, blockIdx.x * kLW + (threadIdx.x >> 5), sm);
+}
+
+// Ensemble: each warp takes one 32-slot block of the concatenated sorted
+// arrays; blocks belong to one simulation (bases are multiples of 32), whose
+// tree, parameters and semantics the walk uses.  Simulations with the other
+// semantics are left to the other instantiation.
+template <bool MASKED>
+__global__ void __launch_bounds__(kLW * 32) k_walk_list_ens(EnsArgs e) {
+  __shared__ ListSmem<MASKED> sm;
+  const int blk = blockIdx.x * kLW + (threadIdx.x >> 5);
+  if (blk >= e.nblocks) return;
+  const int s = e.blk_sim[blk];
+  if (s < 0) return;
+  const SimDesc d = e.sims[s];
+  if (!d.active || d.n < 2 || (d.traverse == NB_TRAVERSE_THREAD) != MASKED) return;
+  WalkArgs a;
+  a.n = d.n;
+  a.ps = e.pos_sorted + d.base;
+  a.perm = e.perm + d.base;
+  a.nodes = e.nodes + d.base;
+  a.theta2 = d.theta2;
+  a.eps2 = d.eps2;
+  a.G = d.G;
+  a.half_dt = d.half_dt;
+  a.acc = e.acc;
+  a.vel = e.kick_after ? e.vel : nullptr;
+  a.counts = nullptr;
+  a.perm_limit = e.nslots;
+  a.err = e.err;
+  walk_list_warp<MASKED, false>(a, blk - d.base / 32, sm);
+}
+
+int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
+  const int blocks = (e.nblocks + kLW - 1) / kLW;
+  if (blocks == 0) return NB_OK;
+  k_walk_list_ens<false><<<blocks, kLW * 32, 0, st>>>(e);
+  k_walk_list_ens<true><<<blocks, kLW * 32, 0, st>>>(e);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
 }
 
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st) {

@@ -162,6 +162,68 @@ struct APGeom {
 };
 APGeom allpairs_geometry(int n);
 
+// ---------------------------------------------------------------------------
+// Ensembles: many simulations in one set of arrays.  Simulation s owns slots
+// [base, base + n) of every per-particle array (original order for the
+// state, Morton order for the sorted arrays and its tree: internal node i at
+// base + i, parent entries at 2 base + id); bases are multiples of 32, so a
+// 32-slot block (one warp) belongs to at most one simulation.  Slots between
+// simulations are unused.
+// ---------------------------------------------------------------------------
+struct SimDesc {
+  int n;          // particles
+  int base;       // first slot, a multiple of 32
+  int coff;       // particles of the simulations before this one
+  int traverse;   // NB_TRAVERSE_*
+  float half_dt, dt, eps2, G, theta2;
+  int active;     // 1: stepped
+  int compensated;
+  int pad;
+};
+
+constexpr int kEnsSimBits = 10;                     // sim id field of the keys
+constexpr int kEnsMaxSims = (1 << kEnsSimBits) - 1; // id 1023 marks unused slots
+constexpr int kEnsKeyBits = 30 + kEnsSimBits;       // 40 bits, 5 sort passes
+
+struct EnsArgs {
+  int nsims;
+  int nslots;                 // slot extent (multiple of 32)
+  int nblocks;                // nslots / 32
+  const SimDesc* sims;
+  const int* blk_sim;         // [nblocks] simulation of each 32-slot block, -1
+  float4* pos;                // state, original order, [nslots]
+  float4* pos_lo;
+  float4* vel;
+  float4* acc;
+  float4* pos_sorted;         // [nslots]
+  uint64_t* keys;             // [nslots] x2: (sim << 30) | morton30
+  uint64_t* keys_alt;
+  uint32_t* perm;             // [nslots] x2: original slot of each sorted slot
+  uint32_t* perm_alt;
+  Node* nodes;                // [nslots]
+  int* parent;                // [2 nslots]
+  int* visit;                 // [nslots]
+  double4* sums;              // [nslots]
+  float4* box_lo;
+  float4* box_hi;
+  int* bbox_min;              // [nsims][4] ordered ints
+  int* bbox_max;              // [nsims][4]
+  uint32_t* hist;             // [8][256] + tile counters + look-back words
+  uint32_t* tile_ctr;
+  uint32_t* status;
+  int status_tiles;
+  unsigned* err;
+  bool kick_drift;
+  bool kick_after;
+};
+
+int launch_ens_prep(const EnsArgs& e, cudaStream_t st);
+int launch_ens_morton(const EnsArgs& e, cudaStream_t st);
+int launch_ens_sort(EnsArgs& e, cudaStream_t st);   // updates e.keys / e.perm
+int launch_ens_build(const EnsArgs& e, cudaStream_t st);
+int launch_ens_com(const EnsArgs& e, cudaStream_t st);
+int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
+
 // A view of a simulation handle's device state (defined in api.cu) for the
 // run loop in io.cu.
 struct SimView {

@@ -20,6 +20,8 @@ struct WalkArgs {
   float4* acc;       // original order
   float4* vel;       // closing kick target (original order) or nullptr
   int* counts;       // debug interaction counts (sorted order) or nullptr
+  int perm_limit;    // permutation values must be below this (n, or the
+                     // ensemble's slot count)
   unsigned* err;
 };
 
@@ -47,7 +49,7 @@ __device__ __forceinline__ void pair_term(float3& a, float dx, float dy,
 // acc[perm[t]] = G a, and the closing kick v += dt/2 acc when vel is set.
 __device__ __forceinline__ void epilogue(const WalkArgs& a, int t, float3 ai) {
   const uint32_t o = a.perm[t];
-  if (o >= (uint32_t)a.n) {   // only after a failed sort (error word set)
+  if (o >= (uint32_t)a.perm_limit) {   // only after a failed sort (error word set)
     raise_err(a.err, NB_DEVERR_SORT);
     return;
   }
@@ -166,5 +168,6 @@ __device__ __forceinline__ float3 dfs_walk_warp(const WalkArgs& a, float4 bi,
 }
 
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st);
+int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
 
 }  // namespace nb
