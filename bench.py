@@ -64,9 +64,15 @@ def parse_args():
                     help="naive: time the all-pairs module instead (e.g. --n 262144)")
     ap.add_argument("--walk", choices=["list", "dfs"], default="list",
                     help="tree-walk kernel: batched list walk or depth-first walk")
-    ap.add_argument("--workload", choices=["single", "ensemble"], default="single",
-                    help="ensemble: batched encounters vs the plain path one at a time")
+    ap.add_argument("--workload", choices=["single", "ensemble", "serve"],
+                    default="single",
+                    help="ensemble: batched encounters vs the plain path one at a "
+                         "time; serve: request stream through the server vs FIFO")
     ap.add_argument("--nsims", type=int, default=512)
+    ap.add_argument("--requests", type=int, default=200)
+    ap.add_argument("--serve-nmax", type=int, default=262144)
+    ap.add_argument("--serve-smax", type=int, default=500)
+    ap.add_argument("--hbm-budget-gb", type=float, default=24.0)
     return ap.parse_args()
 
 
@@ -493,6 +499,125 @@ def run_ensemble(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
+def serve_requests(args, rng):
+    """The request stream: N log-uniform in [4096, nmax], steps U[100, smax],
+    theta from {0.3, 0.5, 0.7}, encounter geometry as the ensemble recipe, a
+    frame every 50 steps."""
+    from nbodyssey_b200 import api, ic
+    import math
+    reqs = []
+    for k in range(args.requests):
+        n = int(round(math.exp(rng.uniform(math.log(4096), math.log(args.serve_nmax)))))
+        spec = dict(n=n, mass_ratio=float(rng.uniform(0.25, 1.0)),
+                    impact=float(rng.uniform(2.0, 8.0)),
+                    inclination_deg=float(rng.uniform(0.0, 90.0)),
+                    approach=float(rng.uniform(0.3, 0.7)),
+                    seed=int(rng.integers(0, 2 ** 31 - 1)))
+        pos, vel = ic.from_spec(spec)
+        prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh",
+                            theta=float(rng.choice([0.3, 0.5, 0.7])),
+                            traverse=args.traverse, walk_kernel=args.walk)
+        steps = int(rng.integers(100, args.serve_smax + 1))
+        reqs.append((pos, vel, prm, steps))
+    return reqs
+
+
+def _pcts(lat):
+    lat = np.asarray(lat)
+    return {"p50": float(np.percentile(lat, 50)), "p95": float(np.percentile(lat, 95)),
+            "p99": float(np.percentile(lat, 99))}
+
+
+def run_serve(args, rank, world, local, pg):
+    """Served request stream vs FIFO one at a time through the plain path.
+    (1) capacity: every request submitted at t=0, particle-steps/s;
+    (2) latency: Poisson arrivals at 80 % of the plain path's capacity, the
+    same arrival times for both, p50/p95/p99 completion latency."""
+    import threading
+    from nbodyssey_b200 import _lib as L
+    from nbodyssey_b200 import api
+    from nbodyssey_b200.server import Server
+    lib = L.load()
+    L.check(lib.nb_set_device(local))
+    rng = np.random.default_rng(1000 + rank)
+    reqs = serve_requests(args, rng)
+    work = float(sum(p.shape[0] * s for p, _, _, s in reqs))
+    budget = int(args.hbm_budget_gb * (1 << 30))
+
+    def plain_one(pos, vel, prm, steps):
+        with api.Simulation(pos, vel, prm) as sim:
+            done = 0
+            while done < steps:   # frames every 50 steps, as the server's
+                k = min(50 - done % 50, steps - done)
+                sim.step(k)
+                done += k
+                sim.positions()
+            sim.velocities()
+
+    def serve_all(arrivals):
+        lat = []
+        with Server(hbm_budget_bytes=budget, max_sims=1023) as srv:
+            t0 = time.perf_counter()
+            ids = []
+            for (pos, vel, prm, steps), ta in zip(reqs, arrivals):
+                d = t0 + ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids.append((srv.submit(pos, vel, prm, steps, dump_every=50),
+                            time.perf_counter()))
+            for rid, ts in ids:
+                srv.wait(rid, 3600)
+                st, t_sub, t_adm, t_done = srv.poll(rid)
+                lat.append(t_done - t_sub)
+                srv.result(rid)
+            wall = time.perf_counter() - t0
+            stats = srv.stats()
+        return wall, lat, stats
+
+    def fifo_all(arrivals):
+        lat = [0.0] * len(reqs)
+        t0 = time.perf_counter()
+        for k, ((pos, vel, prm, steps), ta) in enumerate(zip(reqs, arrivals)):
+            d = t0 + ta - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            plain_one(pos, vel, prm, steps)
+            lat[k] = time.perf_counter() - (t0 + ta)
+        return time.perf_counter() - t0, lat
+
+    plain_one(*reqs[0])                      # warm-up (JIT-free, but pages in)
+    zero = [0.0] * len(reqs)
+    wall_s, _, st = serve_all(zero)
+    wall_f, _ = fifo_all(zero)
+    cap_s = work / wall_s
+    cap_f = work / wall_f
+    lam = 0.8 * cap_f / (work / len(reqs))   # requests per second
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs))).tolist()
+    _, lat_s, st2 = serve_all(arrivals)
+    _, lat_f = fifo_all(arrivals)
+    if rank != 0:
+        return
+    line = {"metric": "served particle-steps/s + p99 vs plain (request stream)",
+            "value": cap_s, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic request stream",
+            "config": {"workload": "%d requests, N log-uniform [4096, %d], steps "
+                                   "U[100, %d], theta {0.3,0.5,0.7}, frame every 50 "
+                                   "steps, HBM budget %.0f GB" %
+                                   (args.requests, args.serve_nmax, args.serve_smax,
+                                    args.hbm_budget_gb),
+                       "particle_steps": work},
+            "plain_fifo_particle_steps_per_s": cap_f,
+            "ratio_vs_plain": cap_s / cap_f,
+            "latency_s": {"served": _pcts(lat_s), "plain_fifo": _pcts(lat_f),
+                          "arrival_rate_per_s": lam,
+                          "load": "80 % of the plain path's capacity"},
+            "server": {"peak_running": st["peak_running"],
+                       "engine_steps": st["engine_steps"], "frames": st["frames"],
+                       "frame_bytes": st["frame_bytes"]}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local, pg = dist_setup()
@@ -501,6 +626,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "ensemble":
             run_ensemble(args, rank, world, local, pg)
+        elif args.workload == "serve":
+            run_serve(args, rank, world, local, pg)
         else:
             run_b200(args, rank, world, local, pg)
     finally:

@@ -238,6 +238,44 @@ NB_API int nb_ensemble_record(nb_ensemble* e, int slot /* 0..15 */);
 NB_API int nb_ensemble_elapsed_ms(nb_ensemble* e, int slot0, int slot1, double* ms);
 
 /* ======================================================================
+ * Request server with continuous batching.  No reference counterpart.
+ * Requests (a simulation state, parameters, a step count, a frame cadence)
+ * are admitted in arrival order whenever their footprint fits the free part
+ * of a slot pool sized by an HBM budget (later requests may pass one that
+ * does not fit yet); all running simulations advance together, one set of
+ * launches per step, and state and trees stay on the device until a request
+ * finishes.  Frames (every dump_every-th step, as src/main.cu:188) stream to
+ * the host on a side stream and, with out_dir, to out_dir/frame_%05d.bin.
+ * Each result is bit-identical to running the request alone.  Barnes-Hut,
+ * 30-bit keys.
+ * ==================================================================== */
+typedef struct nb_server nb_server;
+typedef struct nb_server_stats {
+  long long completed, failed, queued, running, engine_steps;
+  double particle_steps;     /* sum over steps of the particles advanced */
+  long long frames, frame_bytes;
+  double busy_s;             /* host time from the first to the last step */
+  int peak_running;
+  long long capacity_slots, used_slots;
+} nb_server_stats;
+/* hbm_budget_bytes sizes the slot pool (about 224 bytes per particle slot);
+ * max_sims <= 1023 simulations run at once. */
+NB_API int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out);
+/* Stops after the running and queued requests are abandoned; frees all. */
+NB_API int nb_server_destroy(nb_server* s);
+NB_API int nb_server_submit(nb_server* s, int n, const float* pos4, const float* vel4,
+                            const nb_params* p, int steps, int dump_every,
+                            const char* out_dir, long long* id);
+/* state: 0 queued, 1 running, 2 done, 3 failed; seconds since the server
+ * started (admit / done are 0 until they happen). */
+NB_API int nb_server_poll(nb_server* s, long long id, int* state, double* t_submit,
+                          double* t_admit, double* t_done);
+NB_API int nb_server_wait(nb_server* s, long long id, double timeout_s);
+NB_API int nb_server_result(nb_server* s, long long id, float* pos4, float* vel4,
+                            int release);
+NB_API int nb_server_get_stats(nb_server* s, nb_server_stats* out);
+
+/* ======================================================================
  * Files and the run loop (src/main.cu:115-215, docs/FORMATS.md).
  * ==================================================================== */
 /* load_ic (src/main.cu:115-128).  Call with pos4 = vel4 = NULL to get n. */

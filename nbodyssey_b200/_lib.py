@@ -118,6 +118,15 @@ SIGNATURES = {
     "nb_ensemble_energy": (_I, [_P, _P]),
     "nb_ensemble_record": (_I, [_P, _I]),
     "nb_ensemble_elapsed_ms": (_I, [_P, _I, _I, ctypes.POINTER(_D)]),
+    "nb_server_create": (_I, [_SZ, _I, _PP]),
+    "nb_server_destroy": (_I, [_P]),
+    "nb_server_submit": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _I, _I, _S,
+                              ctypes.POINTER(ctypes.c_longlong)]),
+    "nb_server_poll": (_I, [_P, ctypes.c_longlong, ctypes.POINTER(_I),
+                            ctypes.POINTER(_D), ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "nb_server_wait": (_I, [_P, ctypes.c_longlong, _D]),
+    "nb_server_result": (_I, [_P, ctypes.c_longlong, _P, _P, _I]),
+    "nb_server_get_stats": (_I, [_P, _P]),
     "nb_read_ic": (_I, [_S, ctypes.POINTER(_I), _P, _P]),
     "nb_write_ic": (_I, [_S, _I, _P, _P]),
     "nb_write_frame": (_I, [_S, _I, _I, _P]),

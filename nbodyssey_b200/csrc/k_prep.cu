@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kPrepThreads) k_ens_prep(EnsArgs e,
                 (int)0x80000000, (int)0x80000000};
     if (valid) {
       float4 x = e.pos[slot];
-      if (KD) {
+      if (KD && d.active == 1) {
         float4 v = e.vel[slot];
         const float4 ac = e.acc[slot];
         v.x = __fmaf_rn(d.half_dt, ac.x, v.x);

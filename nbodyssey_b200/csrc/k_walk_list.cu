@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list_ens(EnsArgs e) {
   a.G = d.G;
   a.half_dt = d.half_dt;
   a.acc = e.acc;
-  a.vel = e.kick_after ? e.vel : nullptr;
+  a.vel = (e.kick_after && d.active == 1) ? e.vel : nullptr;
   a.counts = nullptr;
   a.perm_limit = e.nslots;
   a.err = e.err;

@@ -176,7 +176,7 @@ struct SimDesc {
   int coff;       // particles of the simulations before this one
   int traverse;   // NB_TRAVERSE_*
   float half_dt, dt, eps2, G, theta2;
-  int active;     // 1: stepped
+  int active;     // 0: skipped; 1: stepped; 2: a(x) only (newly admitted)
   int compensated;
   int pad;
 };
