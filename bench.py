@@ -284,7 +284,7 @@ def measured_peaks():
 def profiled_traffic():
     """Per-launch DRAM bytes of the walk kernel from the committed ncu
     summary (profiles/), if present."""
-    path = os.path.join(ROOT, "profiles", "walk_warp_1m.txt")
+    path = os.path.join(ROOT, "profiles", "walk_list_1m.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
