@@ -1,0 +1,77 @@
+"""Accuracy gates against the FP64 oracle.
+
+* Barnes-Hut theta 0.5 at N = 1,000,000: median relative force error <= 1 %
+  on a seeded 4,096-target subsample (warp and thread walks), and the theta
+  dial ordered (0.3 < 0.5 < 0.7);
+* 1M Barnes-Hut, 200 steps (dt 0.005): |dE/E| <= 2e-4;
+* precision study (262,144 particles with 10 % Plummer cores, eps 0.01,
+  dt 0.002): all-pairs force median < 1e-5 and |dE/E| <= 2e-4 over 500
+  steps; the Barnes-Hut drift is reported (the reference's own Barnes-Hut
+  drifts by 5e-3 .. 1.2e-2, docs/PERFORMANCE.md:94-104).
+"""
+import numpy as np
+import pytest
+
+from nbodyssey_b200 import api, ic
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+
+
+@pytest.fixture(scope="module")
+def one_million():
+    pos, vel = ic.bh_config(1_000_000, seed=0)
+    tg = np.random.default_rng(0).choice(1_000_000, 4096, replace=False)
+    return pos, vel, tg, O.allpairs_f64(pos, 0.05, targets=tg)
+
+
+@pytest.mark.parametrize("traverse", ["warp", "thread"])
+def test_theta_dial_1m(one_million, traverse):
+    pos, vel, tg, exact = one_million
+    med = []
+    for theta in (0.3, 0.5, 0.7):
+        prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh", theta=theta,
+                            traverse=traverse)
+        with api.Simulation(pos, vel, prm) as sim:
+            a = sim.compute_forces()[:, :3].astype(np.float64)
+        med.append(float(np.median(rel(a[tg], exact))))
+    print("median force error theta 0.3/0.5/0.7 (%s):" % traverse, med)
+    assert med[1] <= 0.01
+    assert med[0] < med[1] < med[2]
+
+
+def test_energy_1m_200_steps(one_million):
+    pos, vel, _, _ = one_million
+    prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh", theta=0.5, traverse="warp")
+    with api.Simulation(pos, vel, prm) as sim:
+        e0 = sim.energy()[0]
+        sim.step(200)
+        e1 = sim.energy()[0]
+    drift = abs(e1 - e0) / abs(e0)
+    print("1M BH 200 steps |dE/E| =", drift)
+    assert drift <= 2e-4
+
+
+def test_precision_study():
+    pos, vel = ic.precision_config(262_144, seed=0)
+    tg = np.random.default_rng(1).choice(262_144, 2048, replace=False)
+    exact = O.allpairs_f64(pos, 0.01, targets=tg)
+    res = {}
+    for force in ("naive", "bh"):
+        prm = api.SimParams(dt=0.002, epsilon=0.01, force=force, theta=0.5,
+                            traverse="warp")
+        with api.Simulation(pos, vel, prm) as sim:
+            a = sim.compute_forces()[:, :3].astype(np.float64)
+            r = rel(a[tg], exact)
+            e0 = sim.energy()[0]
+            sim.step(500)
+            e1 = sim.energy()[0]
+        res[force] = (float(np.median(r)), float(np.percentile(r, 99)),
+                      abs(e1 - e0) / abs(e0))
+    print("precision study (median, p99, |dE/E| over 500 steps):", res)
+    assert res["naive"][0] < 1e-5 and res["naive"][2] <= 2e-4
+    assert res["bh"][0] <= 0.01 and res["bh"][2] < 1e-2
