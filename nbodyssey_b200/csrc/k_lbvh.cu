@@ -373,7 +373,23 @@ __device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
                                           unsigned* err) {
   if (i >= n) return;
   const int ni = n - 1;
-  int node = parent[ni + i];
+  // the child this thread has finished: leaf i to begin with; its data stays
+  // in registers, only the sibling's is read after the arrival
+  int me = ni + i;
+  double s[2][4];
+  float l[2][3], h[2][3];
+  {
+    const float4 p = ps[i];
+    const double m = (double)p.w;
+    s[0][0] = __dmul_rn((double)p.x, m);
+    s[0][1] = __dmul_rn((double)p.y, m);
+    s[0][2] = __dmul_rn((double)p.z, m);
+    s[0][3] = m;
+    l[0][0] = h[0][0] = p.x;
+    l[0][1] = h[0][1] = p.y;
+    l[0][2] = h[0][2] = p.z;
+  }
+  int node = parent[me];
   // a valid tree is at most n-1 levels deep; the bound and the range checks
   // only matter if an earlier phase failed (its error word is then set)
   for (int guard = 0; node >= 0; ++guard) {
@@ -381,40 +397,42 @@ __device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
       raise_err(err, NB_DEVERR_STACK);
       return;
     }
+    // fetched before the arrival: the topology (from the build kernel) and a
+    // leaf sibling's position do not change during this kernel
+    const int2 ch = *reinterpret_cast<const int2*>(&nodes[node].left);
+    const int up = parent[node];
+    if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1 ||
+        (ch.x != me && ch.y != me)) {
+      raise_err(err, NB_DEVERR_STACK);
+      return;
+    }
+    const int sib = ch.x == me ? ch.y : ch.x;
+    float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sib >= ni) sp = ps[sib - ni];
     // acq_rel: releases this thread's writes of the child it finished and
     // acquires the sibling's, which the other arrival released
     cuda::atomic_ref<int, cuda::thread_scope_device> arrivals(visit[node]);
     if (arrivals.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
-    const int2 ch = __ldcg((const int2*)&nodes[node].left);
-    if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1) {
-      raise_err(err, NB_DEVERR_STACK);
-      return;
+    if (sib >= ni) {
+      const double m = (double)sp.w;
+      s[1][0] = __dmul_rn((double)sp.x, m);
+      s[1][1] = __dmul_rn((double)sp.y, m);
+      s[1][2] = __dmul_rn((double)sp.z, m);
+      s[1][3] = m;
+      l[1][0] = h[1][0] = sp.x;
+      l[1][1] = h[1][1] = sp.y;
+      l[1][2] = h[1][2] = sp.z;
+    } else {
+      const double2* qp = reinterpret_cast<const double2*>(&sums[sib]);
+      const double2 q0 = __ldcg(qp), q1 = __ldcg(qp + 1);
+      const float4 bl = __ldcg(&box_lo[sib]);
+      const float4 bh = __ldcg(&box_hi[sib]);
+      s[1][0] = q0.x; s[1][1] = q0.y; s[1][2] = q1.x; s[1][3] = q1.y;
+      l[1][0] = bl.x; l[1][1] = bl.y; l[1][2] = bl.z;
+      h[1][0] = bh.x; h[1][1] = bh.y; h[1][2] = bh.z;
     }
-    double s[2][4];
-    float l[2][3], h[2][3];
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      int id = c == 0 ? ch.x : ch.y;
-      if (id >= ni) {
-        float4 p = ps[id - ni];
-        double m = (double)p.w;
-        s[c][0] = __dmul_rn((double)p.x, m);
-        s[c][1] = __dmul_rn((double)p.y, m);
-        s[c][2] = __dmul_rn((double)p.z, m);
-        s[c][3] = m;
-        l[c][0] = h[c][0] = p.x;
-        l[c][1] = h[c][1] = p.y;
-        l[c][2] = h[c][2] = p.z;
-      } else {
-        const double2* qp = reinterpret_cast<const double2*>(&sums[id]);
-        double2 q0 = __ldcg(qp), q1 = __ldcg(qp + 1);
-        float4 bl = __ldcg(&box_lo[id]);
-        float4 bh = __ldcg(&box_hi[id]);
-        s[c][0] = q0.x; s[c][1] = q0.y; s[c][2] = q1.x; s[c][3] = q1.y;
-        l[c][0] = bl.x; l[c][1] = bl.y; l[c][2] = bl.z;
-        h[c][0] = bh.x; h[c][1] = bh.y; h[c][2] = bh.z;
-      }
-    }
+    // IEEE addition and min / max are commutative: which child is left does
+    // not change the bits
     double4 q;
     q.x = __dadd_rn(s[0][0], s[1][0]);
     q.y = __dadd_rn(s[0][1], s[1][1]);
@@ -437,7 +455,11 @@ __device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
     nodes[node].com = com;
     nodes[node].size2 = __fmul_rn(e, e);
     // published by the release half of the next level's fetch_add
-    node = parent[node];
+    s[0][0] = q.x; s[0][1] = q.y; s[0][2] = q.z; s[0][3] = q.w;
+    l[0][0] = lo.x; l[0][1] = lo.y; l[0][2] = lo.z;
+    h[0][0] = hi.x; h[0][1] = hi.y; h[0][2] = hi.z;
+    me = node;
+    node = up;
   }
 }
 

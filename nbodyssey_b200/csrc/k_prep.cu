@@ -115,13 +115,31 @@ __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a) {
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  if (threadIdx.x < 6) {
-    int c = threadIdx.x;
-    int v = __ldcg(a.bbox_part + c);
-    for (int b = 1; b < (int)gridDim.x; ++b) {
-      int u = __ldcg(a.bbox_part + b * 6 + c);
-      v = c < 3 ? min(v, u) : max(v, u);
+  // the whole last block reduces the block partials (min / max are
+  // order-independent, so the result is exact)
+  int q[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000,
+              (int)0x80000000, (int)0x80000000};
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      q[c] = min(q[c], __ldcg(a.bbox_part + b * 6 + c));
+      q[c + 3] = max(q[c + 3], __ldcg(a.bbox_part + b * 6 + c + 3));
     }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    q[c] = __reduce_min_sync(0xffffffffu, q[c]);
+    q[c + 3] = __reduce_max_sync(0xffffffffu, q[c + 3]);
+  }
+  __syncthreads();   // s_red is reused
+  if (lane == 0)
+    for (int c = 0; c < 6; ++c) s_red[warp][c] = q[c];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int c = threadIdx.x;
+    int v = s_red[0][c];
+    for (int w = 1; w < kPrepThreads / 32; ++w)
+      v = c < 3 ? min(v, s_red[w][c]) : max(v, s_red[w][c]);
     a.bbox[c] = v;
   }
   if (threadIdx.x == 0) *a.ticket = 0u;   // ready for the next launch
