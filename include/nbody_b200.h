@@ -48,6 +48,10 @@ extern "C" {
  *      BhTraversal) ------------------------------------------------------- */
 #define NB_FORCE_NAIVE 0      /* ForceMethod::kNaive, tiled all-pairs */
 #define NB_FORCE_BH 1         /* ForceMethod::kBarnesHut, LBVH rebuilt per step */
+#define NB_FORCE_AUTO 2       /* all-pairs below NB_AUTO_CROSSOVER particles,
+                                 Barnes-Hut from there on (the per-step times
+                                 cross near 20k particles on a B200) */
+#define NB_AUTO_CROSSOVER 20000
 #define NB_TRAVERSE_THREAD 0  /* BhTraversal::kThread, one walk per particle */
 #define NB_TRAVERSE_WARP 1    /* BhTraversal::kWarp, one shared walk per warp */
 

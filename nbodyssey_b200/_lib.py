@@ -23,6 +23,8 @@ NB_ERR_NOTFOUND = 7
 
 NB_FORCE_NAIVE = 0
 NB_FORCE_BH = 1
+NB_FORCE_AUTO = 2
+NB_AUTO_CROSSOVER = 20000
 NB_TRAVERSE_THREAD = 0
 NB_TRAVERSE_WARP = 1
 NB_PHASES = 8

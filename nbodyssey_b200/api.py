@@ -17,9 +17,11 @@ from . import _lib as L
 
 
 class ForceMethod:
-    """src/simulation.hpp:4 (kNaive / kBarnesHut)."""
+    """src/simulation.hpp:4 (kNaive / kBarnesHut), plus AUTO: all-pairs below
+    the measured crossover (NB_AUTO_CROSSOVER particles), Barnes-Hut above."""
     NAIVE = "naive"
     BARNES_HUT = "bh"
+    AUTO = "auto"
 
 
 class BhTraversal:
@@ -45,8 +47,8 @@ class SimParams:
     walk_kernel: str = "list"   # "list" (batched, default) or "dfs"
 
     def to_c(self):
-        if self.force not in (ForceMethod.NAIVE, ForceMethod.BARNES_HUT):
-            raise ValueError("force must be naive or bh, got: %r" % self.force)
+        if self.force not in (ForceMethod.NAIVE, ForceMethod.BARNES_HUT, ForceMethod.AUTO):
+            raise ValueError("force must be naive, bh or auto, got: %r" % self.force)
         if self.traverse not in (BhTraversal.THREAD, BhTraversal.WARP):
             raise ValueError("traverse must be thread or warp, got: %r" % self.traverse)
         p = L.nb_params()
@@ -54,7 +56,8 @@ class SimParams:
         p.eps = self.epsilon
         p.G = self.G
         p.theta = self.theta
-        p.force = L.NB_FORCE_BH if self.force == ForceMethod.BARNES_HUT else L.NB_FORCE_NAIVE
+        p.force = {ForceMethod.NAIVE: L.NB_FORCE_NAIVE, ForceMethod.BARNES_HUT: L.NB_FORCE_BH,
+                   ForceMethod.AUTO: L.NB_FORCE_AUTO}[self.force]
         p.traverse = L.NB_TRAVERSE_WARP if self.traverse == BhTraversal.WARP else L.NB_TRAVERSE_THREAD
         p.key_bits = int(self.key_bits)
         p.compensated = 1 if self.compensated else 0

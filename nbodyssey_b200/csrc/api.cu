@@ -154,8 +154,8 @@ static int check_params(const nb_params* p) {
     return set_error(NB_ERR_INVALID, "theta must be >= 0");
   if (!std::isfinite(p->dt) || !std::isfinite(p->G))
     return set_error(NB_ERR_INVALID, "dt and G must be finite");
-  if (p->force != NB_FORCE_NAIVE && p->force != NB_FORCE_BH)
-    return set_error(NB_ERR_INVALID, "force must be NB_FORCE_NAIVE or NB_FORCE_BH");
+  if (p->force != NB_FORCE_NAIVE && p->force != NB_FORCE_BH && p->force != NB_FORCE_AUTO)
+    return set_error(NB_ERR_INVALID, "force must be NB_FORCE_NAIVE, _BH or _AUTO");
   if (p->traverse != NB_TRAVERSE_THREAD && p->traverse != NB_TRAVERSE_WARP)
     return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
   if (p->key_bits != 30 && p->key_bits != 63)
@@ -208,10 +208,17 @@ static int mark(PhaseMarks* pm, int phase, cudaStream_t st) {
   return NB_OK;
 }
 
+// NB_FORCE_AUTO: all-pairs below the measured crossover, Barnes-Hut above.
+static int resolve_force(int force, int n) {
+  if (force != NB_FORCE_AUTO) return force;
+  return n < NB_AUTO_CROSSOVER ? NB_FORCE_NAIVE : NB_FORCE_BH;
+}
+
 // The whole force evaluation (plus the optional fused kick / drift / kick).
 // n < 2 with Barnes-Hut writes zeros as src/forces_bh.cu:466-469 does.
 static int enqueue_forces(Workspace& w, const StepArgs& a, int force,
                           cudaStream_t st, PhaseMarks* pm) {
+  force = resolve_force(force, a.n);
   if (pm) NB_CUDA(cudaEventRecord(pm->start, st));
   if (force == NB_FORCE_BH && a.n < 2) {
     if (a.kick_drift) NB_TRY(launch_prep(w, a, false, false, st));
@@ -403,7 +410,7 @@ static int sim_capture(nb_sim* s) {
   }
   s->graph_valid = false;
   // reserve first so no allocation happens during capture
-  if (s->p.force == NB_FORCE_BH)
+  if (resolve_force(s->p.force, s->n) == NB_FORCE_BH)
     NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
   else
     NB_TRY(ws_reserve_allpairs(s->ws, s->n, allpairs_geometry(s->n).jsplit));
@@ -754,7 +761,7 @@ int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
 int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts) {
   if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
   int* dcounts = nullptr;
-  if (counts && s->p.force == NB_FORCE_BH && s->n >= 2) {
+  if (counts && resolve_force(s->p.force, s->n) == NB_FORCE_BH && s->n >= 2) {
     NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
     dcounts = s->ws.counts;
   }

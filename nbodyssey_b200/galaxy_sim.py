@@ -33,7 +33,7 @@ def parse_args(argv=None):
     ap.add_argument("--eps", type=float, default=0.05)
     ap.add_argument("--G", type=float, default=1.0)
     ap.add_argument("--theta", type=float, default=0.5)
-    ap.add_argument("--force", choices=["naive", "bh"], default="naive")
+    ap.add_argument("--force", choices=["naive", "bh", "auto"], default="naive")
     ap.add_argument("--traverse", choices=["thread", "warp"], default="thread")
     ap.add_argument("--compare-forces", action="store_true")
     ap.add_argument("--key-bits", type=int, choices=[30, 63], default=30)

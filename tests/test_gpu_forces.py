@@ -162,6 +162,22 @@ def test_theta05_accuracy_vs_fp64():
             assert np.median(r) < 0.02
 
 
+@pytest.mark.parametrize("n,expect", [(5_000, "naive"), (30_000, "bh")])
+def test_auto_force_picks_by_crossover(n, expect):
+    """force=auto is the all-pairs module below 20,000 particles and
+    Barnes-Hut from there on, bit for bit."""
+    pos, vel = ic.two_disks(n, seed=18)
+    out = {}
+    for force in ("auto", expect):
+        prm = api.SimParams(dt=0.005, epsilon=EPS, theta=0.5, force=force,
+                            traverse="warp")
+        with api.Simulation(pos, vel, prm) as sim:
+            sim.step(2)
+            out[force] = (sim.positions(), sim.velocities())
+    assert np.array_equal(out["auto"][0], out[expect][0])
+    assert np.array_equal(out["auto"][1], out[expect][1])
+
+
 def test_determinism():
     pos, _ = ic.two_disks(50_000, seed=16)
     a1, _ = bh_forces(pos, 0.5, "warp")
