@@ -260,6 +260,8 @@ static int check_device_error(Workspace& w, cudaStream_t st) {
     std::snprintf(buf, sizeof(buf), "%x", e);
     m += buf;
     if (e & NB_DEVERR_STACK) m += " (tree walk stack overflow)";
+    if (e & NB_DEVERR_TREE) m += " (inconsistent tree in the centre-of-mass pass)";
+    if (e & NB_DEVERR_VISITS) m += " (tree walk visit limit)";
     if (e & NB_DEVERR_SORT) m += " (radix sort look-back wait limit)";
     if (e & NB_DEVERR_WAIT) m += " (bulk-copy barrier wait limit)";
     if (e & NB_DEVERR_QUEUE) m += " (work-queue wait limit)";

@@ -394,16 +394,16 @@ __device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
   // only matter if an earlier phase failed (its error word is then set)
   for (int guard = 0; node >= 0; ++guard) {
     if (node >= ni || guard >= n) {
-      raise_err(err, NB_DEVERR_STACK);
+      raise_err(err, NB_DEVERR_TREE);
       return;
     }
     // fetched before the arrival: the topology (from the build kernel) and a
     // leaf sibling's position do not change during this kernel
-    const int2 ch = *reinterpret_cast<const int2*>(&nodes[node].left);
-    const int up = parent[node];
+    const int2 ch = __ldcg(reinterpret_cast<const int2*>(&nodes[node].left));
+    const int up = __ldcg(&parent[node]);
     if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1 ||
         (ch.x != me && ch.y != me)) {
-      raise_err(err, NB_DEVERR_STACK);
+      raise_err(err, NB_DEVERR_TREE);
       return;
     }
     const int sib = ch.x == me ? ch.y : ch.x;

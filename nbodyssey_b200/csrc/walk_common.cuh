@@ -78,7 +78,7 @@ __device__ __forceinline__ float3 dfs_walk_thread(const WalkArgs& a, float4 bi,
   // a walk of a valid tree visits each of the 2n-1 nodes at most once
   for (int visits = 0;; ++visits) {
     if (visits >= 2 * a.n) {
-      raise_err(a.err, NB_DEVERR_STACK);
+      raise_err(a.err, NB_DEVERR_VISITS);
       break;
     }
     if (id >= ni) {
@@ -129,7 +129,7 @@ __device__ __forceinline__ float3 dfs_walk_warp(const WalkArgs& a, float4 bi,
   int id = 0;
   for (int visits = 0;; ++visits) {
     if (visits >= 2 * a.n) {
-      if (lane == 0) raise_err(a.err, NB_DEVERR_STACK);
+      if (lane == 0) raise_err(a.err, NB_DEVERR_VISITS);
       break;
     }
     if (id >= ni) {
