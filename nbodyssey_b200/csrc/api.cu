@@ -75,6 +75,10 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_TRY(dalloc(&w.nodes, ni));
   NB_TRY(dalloc(&w.parent, 2 * (size_t)cap));
   NB_TRY(dalloc(&w.visit, ni));
+  for (int i = 0; i < 2; ++i) {
+    NB_TRY(dalloc(&w.seg[i], build_seg_entries(cap)));
+    NB_TRY(dalloc(&w.seg_count[i], build_seg_entries(cap)));
+  }
   NB_TRY(dalloc(&w.sums, ni));
   NB_TRY(dalloc(&w.box_lo, ni));
   NB_TRY(dalloc(&w.box_hi, ni));
@@ -133,6 +137,7 @@ int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit) {
 void ws_free(Workspace& w) {
   cudaFree(w.keys); cudaFree(w.keys_alt); cudaFree(w.vals); cudaFree(w.vals_alt);
   cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.parent); cudaFree(w.visit);
+  for (int i = 0; i < 2; ++i) { cudaFree(w.seg[i]); cudaFree(w.seg_count[i]); }
   cudaFree(w.sums); cudaFree(w.box_lo); cudaFree(w.box_hi); cudaFree(w.hist);
   cudaFree(w.bbox); cudaFree(w.bbox_part); cudaFree(w.bbox_ticket);
   cudaFree(w.src); cudaFree(w.part); cudaFree(w.tickets); cudaFree(w.epart);

@@ -1,8 +1,9 @@
 // LBVH build, rebuilt every step (src/forces_bh.cu:190-331):
 //   Morton keys (+ the radix sort's digit histograms, fused)
 //   onesweep LSD radix sort (+ the position gather, fused into the last pass)
-//   Karras radix-tree build
-//   bottom-up centres of mass / boxes / sizes, FP64 mass-weighted sums.
+//   Karras radix tree + bottom-up centres of mass / boxes / sizes (FP64
+//   mass-weighted sums): one fused bottom-up build in levels for a single
+//   tree, the top-down Karras build + climb for the trees of an ensemble.
 #include <cuda/atomic>
 
 #include "nb_internal.cuh"
@@ -336,29 +337,9 @@ __device__ __forceinline__ void karras_node(const K* __restrict__ keys, int n,
   visit[i] = 0;
 }
 
-template <typename K>
-__global__ void __launch_bounds__(256) k_karras(const K* __restrict__ keys,
-                                                int n, Node* nodes, int* parent,
-                                                int* visit) {
-  karras_node<K>(keys, n, blockIdx.x * blockDim.x + threadIdx.x, nodes, parent,
-                 visit);
-}
-
-int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
-  int blocks = (a.n - 1 + 255) / 256;
-  if (blocks < 1) blocks = 1;
-  if (a.key_bits == 63)
-    k_karras<uint64_t><<<blocks, 256, 0, st>>>((const uint64_t*)w.keys, a.n,
-                                               w.nodes, w.parent, w.visit);
-  else
-    k_karras<uint32_t><<<blocks, 256, 0, st>>>((const uint32_t*)w.keys, a.n,
-                                               w.nodes, w.parent, w.visit);
-  NB_CUDA(cudaGetLastError());
-  return NB_OK;
-}
-
 // ---------------------------------------------------------------------------
-// Bottom-up centres of mass (src/forces_bh.cu:281-331): every leaf climbs;
+// Bottom-up centres of mass over a built tree (src/forces_bh.cu:281-331),
+// used by the ensemble trees: every leaf climbs;
 // the first arrival at a node stops, the second combines both children
 // (left first, so the result does not depend on arrival order).  FP64
 // mass-weighted sums; node com = float(sum / mass); box = min/max of the
@@ -463,21 +444,517 @@ __device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
   }
 }
 
-__global__ void __launch_bounds__(256) k_com(const float4* __restrict__ ps, int n,
-                                             Node* nodes,
-                                             const int* __restrict__ parent,
-                                             int* visit, double4* sums,
-                                             float4* box_lo, float4* box_hi,
-                                             unsigned* err) {
-  com_climb(ps, n, blockIdx.x * blockDim.x + threadIdx.x, nodes, parent, visit,
-            sums, box_lo, box_hi, err);
+// ---------------------------------------------------------------------------
+// Single-tree build: the Karras tree and its centres of mass, bottom up
+// (after Apetrei 2014, "Fast and Simple Agglomerative LBVH Construction").
+// With d(s) = delta(s, s + 1) at the split s between sorted leaves s and
+// s + 1, the Karras tree is the Cartesian tree of d (on sorted keys with the
+// index tie-break, d has a unique minimum on every range): a node over leaves
+// [lo, hi] joins the neighbour across the larger of d(lo - 1) and d(hi).  A
+// node that joins to the right (split hi) is its parent's left child and
+// Karras node hi; one that joins to the left is the right child and node lo.
+// Node records, parent links, FP64 sums and boxes are therefore exactly those
+// of the Karras build plus the centre-of-mass climb (the oracle checks them
+// bit for bit).
+//
+// Levels.  A CTA takes a contiguous run of leaves and a sequence of "items"
+// separated by splits: at the first level the items are its 1024 leaves, at
+// later levels the finished subtrees that the CTAs below left between the
+// splits they could not close.  At a split the first of the two children to
+// arrive parks its cell in shared memory and stops, the second merges both
+// and goes on; a node whose parent split is the run's boundary stops there.
+// The climb runs in rounds over a dense list of pending arrivals while there
+// are more of them than threads, then each thread climbs one arrival on its
+// own.  Node records and parent links are written by a sweep at the end.
+// The splits left open (at most one arrival, or the run's right boundary)
+// go to a fixed-size segment per CTA, in order: they are ancestors of the
+// run's two boundary splits, so there are at most 2 x depth + 1 of them
+// (depth < 60 for 30-bit keys, < 93 for 63-bit).  The next level takes
+// (kLevelItems - 1) / segment CTAs' segments per CTA; the level with one CTA
+// closes the root.
+// ---------------------------------------------------------------------------
+constexpr int kLeafGroup = 1024;     // leaves per CTA at the first level
+constexpr int kLevelThreads = 512;
+constexpr int kLevelItems = 2048;    // capacity of a later level's CTA
+constexpr int kSplitEmpty = -1;
+constexpr int kSplitDone = -2;
+
+__host__ __device__ constexpr int level_seg(int key_bits) {
+  return key_bits == 63 ? 192 : 128;
+}
+__host__ __device__ constexpr int level_fan(int key_bits) {
+  return (kLevelItems - 1) / level_seg(key_bits);
+}
+__host__ __device__ constexpr size_t level_smem(int cap) {
+  // cells (FP64 sums, box lo, box hi), meta, positions, deltas, exchange
+  // words, two arrival lists, scan scratch and list counters
+  return (size_t)cap * (32 + 16 + 16 + 16 + 4 + 4 + 8) + (size_t)(cap + 1) * 4 + 40 * 4;
 }
 
-int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st) {
-  int blocks = (a.n + 255) / 256;
-  k_com<<<blocks, 256, 0, st>>>(w.pos_sorted, a.n, w.nodes, w.parent, w.visit,
-                                w.sums, w.box_lo, w.box_hi, w.err);
+struct LevelArgs {
+  int n;
+  const void* keys;                 // first level
+  const float4* __restrict__ ps;
+  Node* nodes;
+  int* parent;
+  double4* sums;
+  float4* box_lo;
+  float4* box_hi;
+  const int2* in_seg;               // later levels: (position, delta) lists
+  const int* in_count;
+  int in_groups;                    // CTAs of the level below
+  long long in_span;                // leaves per CTA of the level below
+  int2* out_seg;                    // nullptr at the last level
+  int* out_count;
+  int seg;                          // segment capacity
+  int fan;                          // segments per CTA
+  unsigned* err;
+};
+
+struct Cell {   // a finished node: FP64 mass-weighted sums and box
+  double4 s;
+  float4 lo, hi;
+};
+
+template <typename K>
+__device__ __forceinline__ int split_delta(const K* __restrict__ keys, int s) {
+  const K x = keys[s] ^ keys[s + 1];
+  if (x) return clz_k(x);
+  return (int)(8 * sizeof(K)) + __clz(s ^ (s + 1));
+}
+
+__device__ __forceinline__ Cell leaf_cell(const float4* __restrict__ ps, int i) {
+  const float4 p = ps[i];
+  const double m = (double)p.w;
+  Cell c;
+  c.s = make_double4(__dmul_rn((double)p.x, m), __dmul_rn((double)p.y, m),
+                     __dmul_rn((double)p.z, m), m);
+  c.lo = c.hi = make_float4(p.x, p.y, p.z, 0.f);
+  return c;
+}
+
+// IEEE addition and min / max are commutative: the order of a and b does not
+// change the bits.
+__device__ __forceinline__ Cell merge(const Cell& a, const Cell& b) {
+  Cell c;
+  c.s = make_double4(__dadd_rn(a.s.x, b.s.x), __dadd_rn(a.s.y, b.s.y),
+                     __dadd_rn(a.s.z, b.s.z), __dadd_rn(a.s.w, b.s.w));
+  c.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y),
+                     fminf(a.lo.z, b.lo.z), 0.f);
+  c.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y),
+                     fmaxf(a.hi.z, b.hi.z), 0.f);
+  return c;
+}
+
+// Node record of internal node id over leaves [lo, hi] split after leaf sc,
+// and the parent links of its two children.
+__device__ __forceinline__ void write_node(const LevelArgs& a, int id, int lo,
+                                           int hi, int sc, const Cell& c) {
+  const int ni = a.n - 1;
+  const int l = sc == lo ? ni + sc : sc;
+  const int r = sc + 1 == hi ? ni + sc + 1 : sc + 1;
+  float4 com;
+  com.x = __double2float_rn(__ddiv_rn(c.s.x, c.s.w));
+  com.y = __double2float_rn(__ddiv_rn(c.s.y, c.s.w));
+  com.z = __double2float_rn(__ddiv_rn(c.s.z, c.s.w));
+  com.w = __double2float_rn(c.s.w);
+  const float e = fmaxf(__fsub_rn(c.hi.x, c.lo.x),
+                        fmaxf(__fsub_rn(c.hi.y, c.lo.y), __fsub_rn(c.hi.z, c.lo.z)));
+  float4* rec = reinterpret_cast<float4*>(&a.nodes[id]);
+  rec[0] = com;
+  reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(__fmul_rn(e, e)), 0);
+  a.parent[l] = id;
+  a.parent[r] = id;
+}
+
+__device__ __forceinline__ void store_cell(const LevelArgs& a, int id, const Cell& c) {
+  a.sums[id] = c.s;
+  a.box_lo[id] = c.lo;
+  a.box_hi[id] = c.hi;
+}
+
+__device__ __forceinline__ Cell load_cell(const LevelArgs& a, int id) {
+  Cell c;
+  const double2* q = reinterpret_cast<const double2*>(&a.sums[id]);
+  const double2 q0 = __ldcg(q), q1 = __ldcg(q + 1);
+  c.s = make_double4(q0.x, q0.y, q1.x, q1.y);
+  c.lo = __ldcg(&a.box_lo[id]);
+  c.hi = __ldcg(&a.box_hi[id]);
+  return c;
+}
+
+// Shared memory of one level CTA with room for `cap` items.
+struct LevelSmem {
+  double4* sum;    // [cap] cells by slot
+  float4* lo;
+  float4* hi;
+  int4* meta;      // [cap] (lo, hi, split leaf, Karras id) of a node formed
+                   // here, Karras id -1 for an item
+  int* pos;        // [cap] leaf position of split k
+  int* delta;      // [cap + 1] delta[k + 1] = d(split k), delta[0] = d of the
+                   // split left of the run
+  int* exch;       // [cap] far item of the first arrival at split k
+  unsigned* list;  // [2][cap] pending arrivals (ia | ib << 16)
+  int* scan;       // [40]
+  __device__ LevelSmem(unsigned char* raw, int cap) {
+    sum = reinterpret_cast<double4*>(raw);
+    lo = reinterpret_cast<float4*>(sum + cap);
+    hi = lo + cap;
+    meta = reinterpret_cast<int4*>(hi + cap);
+    pos = reinterpret_cast<int*>(meta + cap);
+    delta = pos + cap;
+    exch = delta + cap + 1;
+    list = reinterpret_cast<unsigned*>(exch + cap);
+    scan = reinterpret_cast<int*>(list + 2 * cap);
+  }
+};
+
+// Run of leaves [A, B); M splits in its sequence (the last is the right
+// boundary when B < n); items between them.
+struct Run {
+  int A, B, M, items, local;
+  __device__ int item_lo(const LevelSmem& sm, int i) const {
+    return i == 0 ? A : sm.pos[i - 1] + 1;
+  }
+  __device__ int item_hi(const LevelSmem& sm, int i, int ni) const {
+    return i < M ? sm.pos[i] : ni;
+  }
+};
+
+__device__ __forceinline__ void put_cell(const LevelSmem& sm, int slot, const Cell& c) {
+  sm.sum[slot] = c.s;
+  sm.lo[slot] = c.lo;
+  sm.hi[slot] = c.hi;
+}
+
+__device__ __forceinline__ Cell get_cell(const LevelSmem& sm, int slot) {
+  Cell c;
+  c.s = sm.sum[slot];
+  c.lo = sm.lo[slot];
+  c.hi = sm.hi[slot];
+  return c;
+}
+
+// Appends v to list `which` when `push` (warp-aggregated); all lanes call.
+__device__ __forceinline__ void list_push(const LevelSmem& sm, int* count, int which,
+                                          int cap, bool push, unsigned v) {
+  const unsigned mask = __ballot_sync(0xffffffffu, push);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (push) sm.list[which * cap + base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+// A node over items [ia, ib] (leaves [lo, hi], cell c, formed here or an
+// item) that has just been finished: the root and frontier nodes are written
+// out; any other parks its cell in its slot and becomes a pending arrival.
+// Slot = the node's Karras id in item space (right end if it joins to the
+// right, left end otherwise); an item and a node formed later share a slot
+// only when the item is below the node, and the node is written after the
+// item's cell was read.  Returns whether it parked.
+__device__ __forceinline__ bool finish_node(const LevelArgs& a, const LevelSmem& sm,
+                                            const Run& run, int ia, int ib, int lo,
+                                            int hi, int sc, bool formed, const Cell& c) {
+  const int ni = a.n - 1;
+  if (lo == 0 && hi == ni) {   // the root: this run is the whole tree
+    write_node(a, 0, lo, hi, sc, c);
+    a.parent[0] = -1;
+    return false;
+  }
+  const bool right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
+  const int kid = right ? hi : lo;
+  const int k = right ? ib : ia - 1;
+  if (k < 0 || k >= run.local) {   // parent split on the run's boundary
+    if (formed) {
+      write_node(a, kid, lo, hi, sc, c);
+      store_cell(a, kid, c);
+    }
+    return false;
+  }
+  const int slot = right ? ib : ia;
+  put_cell(sm, slot, c);
+  if (formed) sm.meta[slot] = make_int4(lo, hi, sc, kid);
+  return true;
+}
+
+// One pending arrival (items [ia, ib], parked in its slot) climbs until it
+// is the first at a split or finishes.  acq_rel: the exchange publishes this
+// thread's slot writes and acquires the sibling's.
+__device__ __forceinline__ void climb_arrival(const LevelArgs& a, const LevelSmem& sm,
+                                              const Run& run, unsigned d) {
+  const int ni = a.n - 1;
+  int ia = (int)(d & 0xffffu), ib = (int)(d >> 16);
+  int lo = run.item_lo(sm, ia), hi = run.item_hi(sm, ib, ni);
+  bool right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
+  Cell c = get_cell(sm, right ? ib : ia);
+  for (int guard = 0; guard <= run.items; ++guard) {
+    const int k = right ? ib : ia - 1;
+    cuda::atomic_ref<int, cuda::thread_scope_block> word(sm.exch[k]);
+    const int other = word.exchange(right ? ia : ib, cuda::memory_order_acq_rel);
+    if (other == kSplitEmpty) return;
+    if (other < 0 || other >= run.items || (right ? other <= k : other > k)) break;
+    const Cell o = get_cell(sm, right ? k + 1 : k);
+    sm.exch[k] = kSplitDone;
+    if (right) {
+      ib = other;
+      hi = run.item_hi(sm, other, ni);
+    } else {
+      ia = other;
+      lo = run.item_lo(sm, other);
+    }
+    c = merge(c, o);
+    if (!finish_node(a, sm, run, ia, ib, lo, hi, sm.pos[k], true, c)) return;
+    right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
+  }
+  raise_err(a.err, NB_DEVERR_TREE);
+}
+
+template <typename K, bool FIRST>
+__global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int C = FIRST ? kLeafGroup : kLevelItems;
+  const LevelSmem sm(smem_raw, C);
+  const int n = a.n, ni = n - 1, g = blockIdx.x, tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  Run run;
+  if (FIRST) {
+    const K* __restrict__ keys = static_cast<const K*>(a.keys);
+    run.A = g * kLeafGroup;
+    run.B = min(n, run.A + kLeafGroup);
+    run.M = run.B < n ? run.B - run.A : run.B - run.A - 1;
+    for (int k = tid; k < run.M; k += kLevelThreads) {
+      sm.pos[k] = run.A + k;
+      sm.delta[k + 1] = split_delta(keys, run.A + k);
+    }
+    if (tid == 0) sm.delta[0] = run.A > 0 ? split_delta(keys, run.A - 1) : -1;
+  } else {
+    const int r0 = g * a.fan, r1 = min(a.in_groups, r0 + a.fan);
+    if (warp == 0) {   // segment offsets (fan <= 32)
+      const int c = r0 + lane < r1 ? min(a.in_count[r0 + lane], a.seg) : 0;
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      sm.scan[lane] = incl - c;
+      if (lane == 31) sm.scan[32] = incl;
+      if (lane == 0) {   // the last entry below is the split left of this run
+        int d = -1;
+        if (r0 > 0) {
+          const int cp = min(a.in_count[r0 - 1], a.seg);
+          if (cp > 0) d = a.in_seg[(size_t)(r0 - 1) * a.seg + cp - 1].y;
+        }
+        sm.delta[0] = d;
+      }
+    }
+    __syncthreads();
+    run.M = sm.scan[32];
+    // one warp per segment
+    for (int r = r0 + warp; r < r1; r += kLevelThreads / 32) {
+      const int off = sm.scan[r - r0];
+      const int c = sm.scan[r - r0 + 1] - off;
+      for (int e = lane; e < c; e += 32) {
+        const int2 v = a.in_seg[(size_t)r * a.seg + e];
+        sm.pos[off + e] = v.x;
+        sm.delta[off + e + 1] = v.y;
+      }
+    }
+    run.A = (int)min((long long)n, r0 * a.in_span);
+    run.B = (int)min((long long)n, r1 * a.in_span);
+  }
+  run.items = run.B < n ? run.M : run.M + 1;
+  run.local = run.B < n ? run.M - 1 : run.M;
+  for (int k = tid; k < run.M; k += kLevelThreads) sm.exch[k] = kSplitEmpty;
+  for (int j = tid; j < run.items; j += kLevelThreads) sm.meta[j].w = -1;
+  int* count = sm.scan + 34;   // three rotating list counters
+  if (tid < 3) count[tid] = 0;
+  __syncthreads();
+
+  // round 0: every item parks its cell and becomes a pending arrival
+  for (int base = 0; base < run.items; base += kLevelThreads) {
+    const int j = base + tid;
+    bool push = false;
+    if (j < run.items) {
+      const int lo = run.item_lo(sm, j), hi = run.item_hi(sm, j, ni);
+      Cell c;
+      if (FIRST || lo == hi) {
+        c = leaf_cell(a.ps, lo);
+      } else {   // a subtree finished below: its Karras id follows its direction
+        const bool right = lo == 0 || (hi != ni && sm.delta[j + 1] > sm.delta[j]);
+        c = load_cell(a, right ? hi : lo);
+      }
+      push = finish_node(a, sm, run, j, j, lo, hi, -1, false, c);
+    }
+    list_push(sm, &count[0], 0, C, push, (unsigned)j | ((unsigned)j << 16));
+  }
+  __syncthreads();
+
+  // rounds: each pending arrival takes its split's exchange word; the second
+  // of two siblings merges them.  A slot is written at least one barrier
+  // before any exchange that can lead to its read, so relaxed atomics do.
+  // Once no more arrivals are pending than there are threads, each takes one
+  // and climbs on its own (block-scope acq_rel exchanges, no barriers).
+  int cur = 0;
+  for (int round = 0; round <= run.items; ++round) {
+    const int L = count[round % 3];
+    if (L == 0) break;
+    if (L <= kLevelThreads) {
+      if (tid < L) climb_arrival(a, sm, run, sm.list[cur * C + tid]);
+      break;
+    }
+    if (tid == 0) count[(round + 2) % 3] = 0;
+    for (int base = 0; base < L; base += kLevelThreads) {
+      const int i = base + tid;
+      bool push = false;
+      unsigned v = 0;
+      if (i < L) {
+        const unsigned d = sm.list[cur * C + i];
+        int ia = (int)(d & 0xffffu), ib = (int)(d >> 16);
+        int lo = run.item_lo(sm, ia), hi = run.item_hi(sm, ib, ni);
+        const bool right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
+        const int k = right ? ib : ia - 1;
+        const int other = atomicExch(&sm.exch[k], right ? ia : ib);
+        if (other != kSplitEmpty) {
+          if (other < 0 || other >= run.items || (right ? other <= k : other > k)) {
+            raise_err(a.err, NB_DEVERR_TREE);
+          } else {
+            const Cell mine = get_cell(sm, right ? ib : ia);
+            const Cell o = get_cell(sm, right ? k + 1 : k);
+            sm.exch[k] = kSplitDone;
+            if (right) {
+              ib = other;
+              hi = run.item_hi(sm, other, ni);
+            } else {
+              ia = other;
+              lo = run.item_lo(sm, other);
+            }
+            push = finish_node(a, sm, run, ia, ib, lo, hi, sm.pos[k], true, merge(mine, o));
+            v = (unsigned)ia | ((unsigned)ib << 16);
+          }
+        }
+      }
+      list_push(sm, &count[(round + 1) % 3], cur ^ 1, C, push, v);
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  __syncthreads();
+  // node records of the nodes formed here, in slot order
+  for (int j = tid; j < run.items; j += kLevelThreads) {
+    const int4 m = sm.meta[j];
+    if (m.w >= 0) write_node(a, m.w, m.x, m.y, m.z, get_cell(sm, j));
+  }
+  if (!a.out_seg) return;
+  // a formed child waiting at an open split hands its cell to the next level
+  for (int k = tid; k < run.local; k += kLevelThreads) {
+    const int e = sm.exch[k];
+    if (e < 0) continue;
+    const bool left = e <= k;   // the waiting child covers items [e, k]
+    if (left ? e == k : e == k + 1) continue;   // a single item: stored below
+    const int slot = left ? k : k + 1;
+    store_cell(a, sm.meta[slot].w, get_cell(sm, slot));
+  }
+  // open splits in order: (position, delta) into this CTA's segment
+  const int chunk = (run.M + kLevelThreads - 1) / kLevelThreads;
+  const int k0 = min(run.M, tid * chunk), k1 = min(run.M, k0 + chunk);
+  int cnt = 0;
+  for (int k = k0; k < k1; ++k) cnt += (k >= run.local || sm.exch[k] != kSplitDone);
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) sm.scan[warp] = incl;   // the segment offsets are no longer read
+  __syncthreads();
+  int base = 0, total = 0;
+  for (int w = 0; w < kLevelThreads / 32; ++w) {
+    const int v = sm.scan[w];
+    if (w < warp) base += v;
+    total += v;
+  }
+  int off = base + incl - cnt;
+  for (int k = k0; k < k1; ++k) {
+    if (k >= run.local || sm.exch[k] != kSplitDone) {
+      if (off < a.seg) a.out_seg[(size_t)g * a.seg + off] = make_int2(sm.pos[k], sm.delta[k + 1]);
+      ++off;
+    }
+  }
+  if (tid == 0) {
+    a.out_count[g] = min(total, a.seg);
+    if (total > a.seg) raise_err(a.err, NB_DEVERR_TREE);
+  }
+}
+
+static LevelArgs level_args(Workspace& w, const StepArgs& a) {
+  LevelArgs b{};
+  b.n = a.n;
+  b.keys = w.keys;
+  b.ps = w.pos_sorted;
+  b.nodes = w.nodes;
+  b.parent = w.parent;
+  b.sums = w.sums;
+  b.box_lo = w.box_lo;
+  b.box_hi = w.box_hi;
+  b.seg = level_seg(a.key_bits);
+  b.fan = level_fan(a.key_bits);
+  b.err = w.err;
+  return b;
+}
+
+size_t build_seg_entries(int cap) {
+  return (size_t)((cap + kLeafGroup - 1) / kLeafGroup) * level_seg(63);
+}
+
+// First level: leaf groups (the bottom of the tree, most of its nodes).
+int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  LevelArgs b = level_args(w, a);
+  const int groups = (a.n + kLeafGroup - 1) / kLeafGroup;
+  if (groups > 1) {
+    b.out_seg = w.seg[0];
+    b.out_count = w.seg_count[0];
+  }
+  const int smem = (int)level_smem(kLeafGroup);
+  if (a.key_bits == 63) {
+    NB_CUDA(cudaFuncSetAttribute(k_build_level<uint64_t, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_build_level<uint64_t, true><<<groups, kLevelThreads, smem, st>>>(b);
+  } else {
+    NB_CUDA(cudaFuncSetAttribute(k_build_level<uint32_t, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_build_level<uint32_t, true><<<groups, kLevelThreads, smem, st>>>(b);
+  }
   NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+// Later levels: the tree above the leaf groups, up to the root.
+int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st) {
+  LevelArgs b = level_args(w, a);
+  const int smem = (int)level_smem(kLevelItems);
+  NB_CUDA(cudaFuncSetAttribute(k_build_level<uint32_t, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int groups = (a.n + kLeafGroup - 1) / kLeafGroup;
+  long long span = kLeafGroup;
+  int p = 0;
+  while (groups > 1) {
+    const int next = (groups + b.fan - 1) / b.fan;
+    b.in_seg = w.seg[p];
+    b.in_count = w.seg_count[p];
+    b.in_groups = groups;
+    b.in_span = span;
+    b.out_seg = next > 1 ? w.seg[p ^ 1] : nullptr;
+    b.out_count = next > 1 ? w.seg_count[p ^ 1] : nullptr;
+    k_build_level<uint32_t, false><<<next, kLevelThreads, smem, st>>>(b);
+    NB_CUDA(cudaGetLastError());
+    groups = next;
+    span *= b.fan;
+    p ^= 1;
+  }
   return NB_OK;
 }
 

@@ -76,6 +76,8 @@ struct Workspace {
   Node* nodes = nullptr;          // [cap-1]
   int* parent = nullptr;          // [2cap-1]
   int* visit = nullptr;           // [cap-1]
+  int2* seg[2] = {nullptr, nullptr};      // open splits per build CTA,
+  int* seg_count[2] = {nullptr, nullptr}; // ping-pong between levels
   double4* sums = nullptr;        // [cap-1] FP64 mass-weighted sums
   float4* box_lo = nullptr;       // [cap-1]
   float4* box_hi = nullptr;       // [cap-1]
@@ -142,6 +144,7 @@ int launch_prep(Workspace& w, const StepArgs& a, bool bbox, bool pack,
                 cudaStream_t st);
 int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_sort(Workspace& w, const StepArgs& a, cudaStream_t st);
+size_t build_seg_entries(int cap);
 int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_walk(Workspace& w, const StepArgs& a, cudaStream_t st);

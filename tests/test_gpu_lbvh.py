@@ -53,7 +53,9 @@ def test_reference_fixture_bit_exact(golden_dir, bits):
     _assert_tree_equal(t, O.Tree(p4, bits), bits)
 
 
-@pytest.mark.parametrize("n", [2, 3, 31, 33, 1000, 4095, 4096, 4097, 100_003])
+# 1023 .. 3073 straddle the 1024-leaf groups of the bottom-up build
+@pytest.mark.parametrize("n", [2, 3, 31, 33, 1000, 1023, 1024, 1025, 2049, 3073,
+                               4095, 4096, 4097, 100_003])
 @pytest.mark.parametrize("bits", [30, 63])
 def test_sizes_bit_exact(n, bits):
     pos, _ = ic.two_disks(n, seed=n)
@@ -72,8 +74,11 @@ def test_duplicates_and_coincident_points():
         _assert_tree_equal(_device_tree(p, bits), O.Tree(p, bits), bits)
 
 
-def test_all_points_coincident():
-    p = np.zeros((700, 4), np.float32)
+@pytest.mark.parametrize("n", [700, 5000])
+def test_all_points_coincident(n):
+    """One key for every particle: the tree is the index tie-break's alone
+    (5000 spans several build groups)."""
+    p = np.zeros((n, 4), np.float32)
     p[:, :3] = 1.5
     p[:, 3] = 1.0
     _assert_tree_equal(_device_tree(p, 30), O.Tree(p, 30), 30)
