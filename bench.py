@@ -45,7 +45,22 @@ N_DEFAULT = 1_000_000
 FLOP_PER_PAIR = 20          # src/main.cu:203-207 convention
 BUILD_BYTES_PER_PARTICLE = 230   # algorithmic HBM bytes of the tree build
 L2_FLUSH_BYTES = 256 << 20
-BH_KERNELS_PER_STEP = 9     # prep, morton, 4 sort passes, karras, com, walk
+ENS_KERNELS_PER_STEP = 11   # prep, morton, 5 sort passes, karras, com, 2 walks
+
+
+def bh_kernels_per_step(n, key_bits=30):
+    """Kernels of one Barnes-Hut step: prep, Morton keys, the sort passes,
+    the first build level (1024-leaf groups), one launch per later build
+    level (15 segments per CTA with 30-bit keys, 10 with 63-bit; the
+    geometry of nbodyssey_b200/csrc/k_lbvh.cu) and the walk."""
+    passes = 4 if key_bits == 30 else 8
+    fan = 15 if key_bits == 30 else 10
+    groups = (n + 1023) // 1024
+    levels = 0
+    while groups > 1:
+        groups = (groups + fan - 1) // fan
+        levels += 1
+    return 1 + 1 + passes + 1 + levels + 1
 
 
 def parse_args():
@@ -73,6 +88,9 @@ def parse_args():
     ap.add_argument("--serve-nmax", type=int, default=262144)
     ap.add_argument("--serve-smax", type=int, default=500)
     ap.add_argument("--hbm-budget-gb", type=float, default=24.0)
+    ap.add_argument("--shard", action="store_true",
+                    help="one simulation split over the --gpus ranks (strong "
+                         "scaling) instead of one independent simulation per rank")
     return ap.parse_args()
 
 
@@ -388,7 +406,9 @@ def run_b200(args, rank, world, local, pg):
         "graph_steps_per_s_no_flush": world * args.steps / (graph_ms * 1e-3),
         "phases_ms_per_step": {k: v / calls for k, v in phases.items() if v > 0},
         "interactions_per_particle": inter / n,
-        "gpu_launches": (BH_KERNELS_PER_STEP if args.force == "bh" else 2) * args.steps,
+        # the step's kernels plus the L2-flush kernel before each step
+        "gpu_launches": ((bh_kernels_per_step(n) if args.force == "bh" else 2) + 1)
+                        * args.steps,
         "e2e": {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
                 "path": "nb_set_state_acc + nb_step + nb_get_{positions,"
@@ -418,6 +438,98 @@ def run_b200(args, rank, world, local, pg):
         line.pop("interactions_per_particle")
     if world == 1 and not args.no_cpu_baseline and args.force == "bh":
         line["cpu_baseline"] = cpu_baseline(args)
+    print(json.dumps(line), flush=True)
+
+
+def run_shard(args, rank, world, local, pg):
+    """One Barnes-Hut simulation split over the ranks (nbodyssey_b200/shard.py):
+    every rank builds the whole tree, walks its Morton range of targets, and
+    one NCCL all-gather of sorted accelerations completes each step.  Steps
+    timed with CUDA events on the current stream, max over ranks; L2 flushed
+    (256 MB write) before every timed step."""
+    import torch
+    from nbodyssey_b200 import _lib as L
+    from nbodyssey_b200 import api, ic
+    from nbodyssey_b200.shard import ShardedSimulation
+    lib = L.load()
+    L.check(lib.nb_set_device(local))
+    torch.cuda.set_device(local)
+    params = api.SimParams(dt=0.005, epsilon=0.05, theta=args.theta, force="bh",
+                           traverse=args.traverse, key_bits=30, compensated=True,
+                           walk_kernel=args.walk)
+    n = args.n
+    pos, vel = ic.bh_config(n, seed=0)   # the same simulation on every rank
+    with api.Simulation(pos, vel, params) as one:
+        inter = interactions(one, api, params)
+    sim = ShardedSimulation(pos, vel, params)
+    sim.step(args.warmup)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    dist_barrier(pg)
+    clocks.start()
+    for e0, e1 in evs:
+        flush.zero_()
+        e0.record()
+        sim.step(1)
+        e1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = dist_max(pg, sum(e0.elapsed_time(e1) for e0, e1 in evs))
+
+    # end to end: this rank's whole state in from pinned host memory, one
+    # step, state out
+    eng = sim.engine
+    hp = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    hv, ha = torch.empty_like(hp).pin_memory(), torch.empty_like(hp).pin_memory()
+    hp.copy_(eng.pos); hv.copy_(eng.vel); ha.copy_(eng.acc)
+    for it in range(args.e2e_steps + 2):
+        if it == 2:
+            torch.cuda.synchronize()
+            dist_barrier(pg)
+            t0 = time.perf_counter()
+        eng.pos.copy_(hp, non_blocking=True)
+        eng.vel.copy_(hv, non_blocking=True)
+        eng.acc.copy_(ha, non_blocking=True)
+        sim.step(1)
+        hp.copy_(eng.pos, non_blocking=True)
+        hv.copy_(eng.vel, non_blocking=True)
+        ha.copy_(eng.acc, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = dist_max(pg, time.perf_counter() - t0)
+    sim.close()
+    if rank != 0:
+        return
+    value = args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded two exponential disks (as the default run)",
+        "config": dict(workload(args),
+                       parallelism="one simulation split over %d GPUs: tree built "
+                                   "on every GPU, walk split by Morton range, NCCL "
+                                   "all-gather of sorted accelerations" % world),
+        "particle_steps_per_s": value * n,
+        "interactions_per_particle": inter / n,
+        # per step: the step's kernels on each rank plus the gather kernel
+        # (the flush and the all-gather are torch / NCCL kernels)
+        "gpu_launches": world * (bh_kernels_per_step(n) + 1) * args.steps,
+        "e2e": {"value": args.e2e_steps / e2e_s, "unit": "steps/s",
+                "h2d_bytes_per_step": 48 * n * world, "d2h_bytes_per_step": 48 * n * world,
+                "path": "each rank: pinned host state in, ShardedSimulation.step, "
+                        "state out, wall clock"},
+        "roofline": {"kernel": "whole step (split walk)", "bound": "fp32",
+                     "achieved": FLOP_PER_PAIR * inter / (total_ms / args.steps * 1e-3) / 1e12,
+                     "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                     "work": "20 flop x per-thread-criterion interactions (%.4g per "
+                             "step) over the whole step; the walk alone is in the "
+                             "default (unsplit) line" % inter},
+        "clocks": clk,
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -495,7 +607,7 @@ def run_ensemble(args, rank, world, local, pg):
             "ratio_vs_plain_device": value / plain,
             "wall_s": {"batched": wall_b, "plain_fifo": wall_p,
                        "ratio": wall_p / wall_b},
-            "gpu_launches": BH_KERNELS_PER_STEP + 3}
+            "gpu_launches": ENS_KERNELS_PER_STEP * K}
     print(json.dumps(line), flush=True)
 
 
@@ -628,6 +740,8 @@ def main():
             run_ensemble(args, rank, world, local, pg)
         elif args.workload == "serve":
             run_serve(args, rank, world, local, pg)
+        elif args.shard:
+            run_shard(args, rank, world, local, pg)
         else:
             run_b200(args, rank, world, local, pg)
     finally:

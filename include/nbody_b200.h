@@ -211,6 +211,27 @@ NB_API int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_
 NB_API int nb_compute_forces_naive_static(int n, const float* d_pos4,
                                           float* d_acc4, float eps, float G,
                                           void* stream);
+/* No counterpart in the reference (one process drives one GPU there).  One
+ * rank's share of compute_forces (src/forces.cuh:8) for a simulation split
+ * over several GPUs: every rank holds the whole state and builds the whole
+ * tree, then walks only the sorted targets [t0, t1) (t0 and t1 multiples of
+ * 32, or n) and writes d_part4[t - t0] = a of sorted target t.  With
+ * d_vel4 set, the opening kick (by d_acc4 = a(x)) and the drift of every
+ * particle run first, as in nb_leapfrog_step_dev; d_pos_lo4 (or NULL) holds
+ * the low-order position parts of the compensated drift.  Barnes-Hut only
+ * (NB_FORCE_BH, or NB_FORCE_AUTO that resolves to it).  Asynchronous. */
+NB_API int nb_forces_range_dev(nb_workspace* w, int n, float* d_pos4,
+                               float* d_pos_lo4, float* d_vel4,
+                               const float* d_acc4, float* d_part4,
+                               const nb_params* p, int t0, int t1, void* stream);
+/* Completes a split step once the ranks' parts are concatenated in sorted
+ * order (d_sorted4, n rows): d_acc4[perm[t]] = d_sorted4[t] with the
+ * permutation of this workspace's last nb_forces_range_dev call, and with
+ * d_vel4 set the closing kick.  Bit-identical to the unsplit step.
+ * Asynchronous. */
+NB_API int nb_forces_gather_dev(nb_workspace* w, int n, const float* d_sorted4,
+                                float* d_acc4, float* d_vel4, const nb_params* p,
+                                void* stream);
 /* total_energy(sys, p) (src/integrator.cuh:21): synchronous, e3 on host. */
 NB_API int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,
                         const float* d_vel4, const nb_params* p, double* e3,

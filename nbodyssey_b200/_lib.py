@@ -109,6 +109,9 @@ SIGNATURES = {
     "nb_leapfrog_step_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_total_energy_dev": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _P, _P]),
     "nb_compute_forces_naive_static": (_I, [_I, _P, _P, _F, _F, _P]),
+    "nb_forces_range_dev": (_I, [_P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(nb_params),
+                                 _I, _I, _P]),
+    "nb_forces_gather_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_ensemble_create": (_I, [_I, _P, _P, _P, _P, _PP]),
     "nb_ensemble_destroy": (_I, [_P]),
     "nb_ensemble_size": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_longlong)]),

@@ -195,6 +195,9 @@ static StepArgs make_args(int n, float4* pos, float4* lo, float4* vel,
   a.kick_drift = false;
   a.kick_after = false;
   a.counts = nullptr;
+  a.t0 = 0;
+  a.t1 = n;
+  a.part = nullptr;
   return a;
 }
 
@@ -863,6 +866,49 @@ int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_vel4,
   a.kick_drift = true;
   a.kick_after = true;
   return enqueue_forces(w->ws, a, p->force, (cudaStream_t)stream, nullptr);
+}
+
+int nb_forces_range_dev(nb_workspace* w, int n, float* d_pos4, float* d_pos_lo4,
+                        float* d_vel4, const float* d_acc4, float* d_part4,
+                        const nb_params* p, int t0, int t1, void* stream) {
+  if (!w || !d_pos4 || !d_part4) return set_error(NB_ERR_INVALID, "NULL argument");
+  if (d_vel4 && !d_acc4)
+    return set_error(NB_ERR_INVALID, "the opening kick needs d_acc4 = a(x)");
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  if (resolve_force(p->force, n) != NB_FORCE_BH)
+    return set_error(NB_ERR_INVALID, "a target range needs Barnes-Hut forces");
+  if (t0 < 0 || t1 < t0 || t1 > n || ((t0 & 31) && t0 != n) || ((t1 & 31) && t1 != n))
+    return set_error(NB_ERR_INVALID,
+                     "need 0 <= t0 <= t1 <= n, t0 and t1 multiples of 32 or n");
+  StepArgs a = make_args(n, (float4*)d_pos4, (float4*)d_pos_lo4, (float4*)d_vel4,
+                         (float4*)d_acc4, *p);
+  a.kick_drift = d_vel4 != nullptr;
+  a.t0 = t0;
+  a.t1 = t1;
+  a.part = (float4*)d_part4;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n < 2) {   // no tree: a = 0 (src/forces_bh.cu:466-469)
+    NB_TRY(ws_basic(w->ws));
+    if (a.kick_drift) NB_TRY(launch_prep(w->ws, a, false, false, st));
+    if (t1 > t0) NB_CUDA(cudaMemsetAsync(d_part4, 0, sizeof(float4) * (t1 - t0), st));
+    return NB_OK;
+  }
+  return enqueue_forces(w->ws, a, NB_FORCE_BH, st, nullptr);
+}
+
+int nb_forces_gather_dev(nb_workspace* w, int n, const float* d_sorted4,
+                         float* d_acc4, float* d_vel4, const nb_params* p,
+                         void* stream) {
+  if (!w || !d_sorted4 || !d_acc4) return set_error(NB_ERR_INVALID, "NULL argument");
+  NB_TRY(check_n(n));
+  NB_TRY(check_params(p));
+  if (n >= 2 && w->ws.cap < n)
+    return set_error(NB_ERR_INVALID, "no tree of this size in the workspace");
+  NB_TRY(ws_basic(w->ws));
+  StepArgs a = make_args(n, nullptr, nullptr, (float4*)d_vel4, (float4*)d_acc4, *p);
+  return launch_gather_part(w->ws, a, (const float4*)d_sorted4, n >= 2,
+                            (cudaStream_t)stream);
 }
 
 int nb_total_energy_dev(nb_workspace* w, int n, const float* d_pos4,

@@ -17,8 +17,8 @@ namespace nb {
 // --- per-thread walk (src/forces_bh.cu:335-377) -----------------------------
 template <bool COUNT>
 __global__ void __launch_bounds__(256) k_walk_thread(WalkArgs a) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
+  const int t = a.t0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.t1) return;
   int cnt = 0;
   float3 ai = dfs_walk_thread<COUNT>(a, a.ps[t], &cnt);
   epilogue(a, t, ai);
@@ -30,8 +30,8 @@ template <bool COUNT>
 __global__ void __launch_bounds__(256) k_walk_warp(WalkArgs a) {
   __shared__ int s_stack[256 / 32][kStack];
   const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t - lane >= a.n) return;   // whole warp past the end
+  const int t = a.t0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t - lane >= a.t1) return;   // whole warp past the end of the range
   const bool live = t < a.n;
   int cnt = 0;
   float3 ai = dfs_walk_warp<COUNT>(a, a.ps[live ? t : a.n - 1], live,
@@ -40,6 +40,38 @@ __global__ void __launch_bounds__(256) k_walk_warp(WalkArgs a) {
     epilogue(a, t, ai);
     if (COUNT) a.counts[t] = cnt;
   }
+}
+
+// --- the walk's sorted-order parts back to original order -------------------
+// Same float operations as epilogue(): the result equals the fused walk's.
+__global__ void __launch_bounds__(256) k_gather_part(const float4* __restrict__ sorted,
+                                                     const uint32_t* __restrict__ perm,
+                                                     int n, float half_dt, float4* acc,
+                                                     float4* vel, unsigned* err) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t o = perm ? perm[t] : (uint32_t)t;
+  if (o >= (uint32_t)n) {
+    raise_err(err, NB_DEVERR_SORT);
+    return;
+  }
+  const float4 g = sorted[t];
+  acc[o] = make_float4(g.x, g.y, g.z, 0.f);
+  if (vel) {
+    float4 v = vel[o];
+    v.x = __fmaf_rn(half_dt, g.x, v.x);
+    v.y = __fmaf_rn(half_dt, g.y, v.y);
+    v.z = __fmaf_rn(half_dt, g.z, v.z);
+    vel[o] = v;
+  }
+}
+
+int launch_gather_part(Workspace& w, const StepArgs& a, const float4* sorted,
+                       bool use_perm, cudaStream_t st) {
+  k_gather_part<<<(a.n + 255) / 256, 256, 0, st>>>(sorted, use_perm ? w.vals : nullptr,
+                                                   a.n, a.half_dt, a.acc, a.vel, w.err);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
 }
 
 int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
@@ -57,9 +89,13 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
   a.counts = s.counts;
   a.perm_limit = s.n;
   a.err = w.err;
+  a.t0 = s.t0;
+  a.t1 = s.t1;
+  a.part = s.part;
   if (s.walk_kernel == 0)
     return launch_walk_list(a, s.traverse == NB_TRAVERSE_THREAD, st);
-  int blocks = (s.n + 255) / 256;
+  int blocks = (s.t1 - s.t0 + 255) / 256;
+  if (blocks == 0) return NB_OK;
   if (s.traverse == NB_TRAVERSE_WARP) {
     if (s.counts) k_walk_warp<true><<<blocks, 256, 0, st>>>(a);
     else k_walk_warp<false><<<blocks, 256, 0, st>>>(a);

@@ -71,7 +71,7 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int n = a.n, ni = n - 1;
-  if (wg * 32 >= n) return;   // whole warp past the end
+  if (wg * 32 >= a.t1) return;   // whole warp past the end of the range
   const int t = wg * 32 + lane;
   const bool live = t < n;
   const unsigned live_mask = __ballot_sync(full, live);
@@ -293,7 +293,7 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
 template <bool MASKED, bool COUNT>
 __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
   __shared__ ListSmem<MASKED> sm;
-  walk_list_warp<MASKED, COUNT>(a, blockIdx.x * kLW + (threadIdx.x >> 5), sm);
+  walk_list_warp<MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * kLW + (threadIdx.x >> 5), sm);
 }
 
 // Ensemble: each warp takes one 32-slot block of the concatenated sorted
@@ -323,6 +323,9 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list_ens(EnsArgs e) {
   a.counts = nullptr;
   a.perm_limit = e.nslots;
   a.err = e.err;
+  a.t0 = 0;
+  a.t1 = d.n;
+  a.part = nullptr;
   walk_list_warp<MASKED, false>(a, blk - d.base / 32, sm);
 }
 
@@ -336,7 +339,8 @@ int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
 }
 
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st) {
-  const int warps = (a.n + 31) / 32;
+  const int warps = (a.t1 - a.t0 + 31) / 32;
+  if (warps <= 0) return NB_OK;
   const int blocks = (warps + kLW - 1) / kLW;
   if (masked) {
     if (a.counts) k_walk_list<true, true><<<blocks, kLW * 32, 0, st>>>(a);

@@ -137,6 +137,10 @@ struct StepArgs {
   bool kick_drift;  // opening kick + drift before the force evaluation
   bool kick_after;  // closing kick fused into the force epilogue
   int* counts;      // debug: interactions per sorted target, or nullptr
+  // Barnes-Hut: the walk covers sorted targets [t0, t1); with `part` set it
+  // writes part[t - t0] = a of sorted target t (no kick) instead of `acc`
+  int t0, t1;
+  float4* part;
 };
 
 // prep: [kick + drift] [+ bbox] [+ pack all-pairs sources] [+ zero sort scratch]
@@ -148,6 +152,10 @@ size_t build_seg_entries(int cap);
 int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_walk(Workspace& w, const StepArgs& a, cudaStream_t st);
+// acc[perm[t]] = sorted[t] (+ the closing kick when a.vel is set); the
+// permutation of the workspace's last tree, or the identity without one
+int launch_gather_part(Workspace& w, const StepArgs& a, const float4* sorted,
+                       bool use_perm, cudaStream_t st);
 int launch_allpairs(Workspace& w, const StepArgs& a, cudaStream_t st);
 // energy: {E, KE, PE, Px, Py, Pz} into w.eout (device); positions hi (+lo
 // for the kinetic part is not needed).

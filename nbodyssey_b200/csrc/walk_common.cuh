@@ -23,6 +23,10 @@ struct WalkArgs {
   int perm_limit;    // permutation values must be below this (n, or the
                      // ensemble's slot count)
   unsigned* err;
+  // sorted targets [t0, t1) are walked (multiples of 32, or n); with `part` set, part[t - t0] = G a of sorted target t instead of
+  // the original-order output and the kick
+  int t0, t1;
+  float4* part;
 };
 
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
@@ -48,6 +52,10 @@ __device__ __forceinline__ void pair_term(float3& a, float dx, float dy,
 
 // acc[perm[t]] = G a, and the closing kick v += dt/2 acc when vel is set.
 __device__ __forceinline__ void epilogue(const WalkArgs& a, int t, float3 ai) {
+  if (a.part) {
+    a.part[t - a.t0] = make_float4(a.G * ai.x, a.G * ai.y, a.G * ai.z, 0.f);
+    return;
+  }
   const uint32_t o = a.perm[t];
   if (o >= (uint32_t)a.perm_limit) {   // only after a failed sort (error word set)
     raise_err(a.err, NB_DEVERR_SORT);
