@@ -98,14 +98,17 @@ int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Onesweep LSD radix sort (Adinets & Merrill, 2022), 8-bit digits, stable.
 // Per pass one kernel: each CTA takes the next tile by ticket (so it only
-// waits on CTAs that are already running), ranks its keys with warp-level
-// match/popc, publishes its digit counts, resolves its global offsets by a
-// decoupled look-back over earlier tiles (bounded waits), and scatters.
+// waits on CTAs that are already running), ranks its keys with warp ballots
+// per digit bit, publishes its digit counts, resolves its global offsets by a
+// decoupled look-back over earlier tiles (bounded waits), stages the tile in
+// digit order in shared memory and writes each digit's run contiguously.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kValMask = (1u << 30) - 1u;
 constexpr int kLookbackSpin = 1 << 20;
+constexpr int kLookbackWindow = 4;   // predecessor tiles read per look-back step
+constexpr int kSortBatch = 4;   // staged elements a thread stores together
 
 __device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
   uint32_t v;
@@ -123,8 +126,22 @@ constexpr int kSortMid = 0;
 constexpr int kSortLast = 1;
 constexpr int kSortLastEnsemble = 2;
 
+// Lanes of the warp whose (valid) item has the same 8-bit digit: one ballot
+// per digit bit, so the cost does not grow with the number of distinct
+// digits in the warp.  Meaningful for lanes with ok set.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
+  uint32_t m = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t v = __ballot_sync(0xffffffffu, bit);
+    m &= bit ? v : ~v;
+  }
+  return m;
+}
+
 template <typename K, int MODE>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 2)
     k_sort_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                 K* __restrict__ kout, uint32_t* __restrict__ vout, int n,
                 int shift, const uint32_t* __restrict__ hist,
@@ -134,8 +151,14 @@ __global__ void __launch_bounds__(kSortThreads)
   constexpr int W = kSortThreads / 32;
   __shared__ uint32_t s_wc[W][kSortRadix];
   __shared__ uint32_t s_base[kSortRadix];
+  __shared__ uint32_t s_tex[kSortRadix];
   __shared__ uint32_t s_scan[W];
+  __shared__ uint32_t s_tsc[W];
   __shared__ int s_tile;
+  // the tile in digit order, staged for coalesced stores (dynamic)
+  extern __shared__ __align__(16) unsigned char s_stage[];
+  K* s_key = reinterpret_cast<K*>(s_stage);
+  uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key + kSortTile);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
   for (int i = tid; i < W * kSortRadix; i += kSortThreads) (&s_wc[0][0])[i] = 0u;
@@ -171,8 +194,8 @@ __global__ void __launch_bounds__(kSortThreads)
   for (int k = 0; k < kSortItems; ++k) {
     long idx = seg + k * 32 + lane;
     bool ok = idx < n;
-    uint32_t d = ok ? (uint32_t)((key[k] >> shift) & 0xffu) : 256u;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
+    uint32_t d = ok ? (uint32_t)((key[k] >> shift) & 0xffu) : 0u;
+    uint32_t peers = digit_peers(d, ok);
     uint32_t old = 0;
     if (ok) {
       old = s_wc[warp][d];
@@ -193,59 +216,142 @@ __global__ void __launch_bounds__(kSortThreads)
     run += c;
   }
   const uint32_t count = run;
+  // tile-local start of digit tid in digit order
+  uint32_t tin = count;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, tin, o);
+    if (lane >= o) tin += y;
+  }
+  if (lane == 31) s_tsc[warp] = tin;
   uint32_t* my = status + (size_t)tile * kSortRadix + tid;
   uint32_t excl = 0;
   if (tile == 0) {
     st_relaxed(my, kFlagInc | count);
   } else {
     st_relaxed(my, kFlagAgg | count);
-    for (int t = tile - 1; t >= 0; --t) {
-      const uint32_t* p = status + (size_t)t * kSortRadix + tid;
-      uint32_t s = ld_relaxed(p);
-      int spins = 0;
-      while ((s & ~kValMask) == 0u && spins < kLookbackSpin) {
-        if (spins > 64) __nanosleep(64);
-        s = ld_relaxed(p);
-        ++spins;
+    // kLookbackWindow predecessors' status words are read together, then
+    // taken in order until an inclusive prefix; a tile that has published
+    // nothing yet is waited for (bounded)
+    bool done = false;
+    for (int t = tile - 1; t >= 0 && !done; t -= kLookbackWindow) {
+      uint32_t win[kLookbackWindow];
+#pragma unroll
+      for (int j = 0; j < kLookbackWindow; ++j)
+        win[j] = t - j >= 0 ? ld_relaxed(status + (size_t)(t - j) * kSortRadix + tid)
+                            : kFlagInc;   // before tile 0: an empty prefix
+#pragma unroll
+      for (int j = 0; j < kLookbackWindow; ++j) {
+        if (done) break;
+        uint32_t s = win[j];
+        if ((s & ~kValMask) == 0u) {
+          const uint32_t* p = status + (size_t)(t - j) * kSortRadix + tid;
+          int spins = 0;
+          while ((s & ~kValMask) == 0u && spins < kLookbackSpin) {
+            if (spins > 64) __nanosleep(64);
+            s = ld_relaxed(p);
+            ++spins;
+          }
+          if ((s & ~kValMask) == 0u) {   // gave up: flag it and stop waiting
+            raise_err(err, NB_DEVERR_SORT);
+            done = true;
+            break;
+          }
+        }
+        excl += s & kValMask;
+        if ((s & kFlagInc) != 0u) done = true;
       }
-      if ((s & ~kValMask) == 0u) {   // gave up: flag it and stop waiting
-        raise_err(err, NB_DEVERR_SORT);
-        break;
-      }
-      excl += s & kValMask;
-      if ((s & kFlagInc) != 0u) break;
     }
     st_relaxed(my, kFlagInc | ((excl + count) & kValMask));
   }
-  s_base[tid] = gexcl + excl;
+  __syncthreads();   // s_tsc
+  uint32_t tofs = 0;
+  for (int i = 0; i < warp; ++i) tofs += s_tsc[i];
+  const uint32_t texcl = tofs + tin - count;
+  s_tex[tid] = texcl;
+  // global index of tile-local digit-order index i of digit d: s_base[d] + i
+  // (unsigned wrap-around cancels)
+  s_base[tid] = gexcl + excl - texcl;
   __syncthreads();
 
 #pragma unroll
   for (int k = 0; k < kSortItems; ++k) {
     long idx = seg + k * 32 + lane;
     if (idx < n) {
-      uint32_t d = (uint32_t)((key[k] >> shift) & 0xffu);
-      uint32_t dst = s_base[d] + s_wc[warp][d] + rank[k];
-      if (dst < (uint32_t)n && val[k] < (uint32_t)n) {
-        if (MODE == kSortLastEnsemble) {
-          // keys arrive grouped by simulation (id in bits 30+); rank d within
-          // the group goes to slot base + (d - coff); unused slots drop out
-          const uint32_t s = (uint32_t)(key[k] >> 30);
-          if (s >= (uint32_t)nsims) continue;
-          dst = (uint32_t)sims[s].base + (dst - (uint32_t)sims[s].coff);
-          if (dst >= (uint32_t)n) {
-            raise_err(err, NB_DEVERR_SORT);
-            continue;
-          }
-        }
-        kout[dst] = key[k];
-        vout[dst] = val[k];
-        if (MODE != kSortMid) pos_sorted[dst] = pos[val[k]];
+      const uint32_t d = (uint32_t)((key[k] >> shift) & 0xffu);
+      const uint32_t lpos = s_tex[d] + s_wc[warp][d] + rank[k];
+      if (lpos < (uint32_t)kSortTile) {
+        s_key[lpos] = key[k];
+        s_val[lpos] = val[k];
       } else {
         raise_err(err, NB_DEVERR_SORT);
       }
     }
   }
+  __syncthreads();
+  // kSortBatch elements per thread at a time, so that the last pass's
+  // position gathers are in flight together
+  const int tn = (int)min((long)kSortTile, (long)n - (long)tile * kSortTile);
+  for (int base = tid; base < tn; base += kSortBatch * kSortThreads) {
+    K kk[kSortBatch];
+    uint32_t vv[kSortBatch], dst[kSortBatch];
+    bool put[kSortBatch];
+#pragma unroll
+    for (int j = 0; j < kSortBatch; ++j) {
+      const int i = base + j * kSortThreads;
+      put[j] = false;
+      if (i >= tn) continue;
+      kk[j] = s_key[i];
+      vv[j] = s_val[i];
+      const uint32_t d = (uint32_t)((kk[j] >> shift) & 0xffu);
+      dst[j] = s_base[d] + (uint32_t)i;
+      if (dst[j] >= (uint32_t)n || vv[j] >= (uint32_t)n) {
+        raise_err(err, NB_DEVERR_SORT);
+        continue;
+      }
+      if (MODE == kSortLastEnsemble) {
+        // keys arrive grouped by simulation (id in bits 30+); rank d within
+        // the group goes to slot base + (d - coff); unused slots drop out
+        const uint32_t s = (uint32_t)(kk[j] >> 30);
+        if (s >= (uint32_t)nsims) continue;
+        dst[j] = (uint32_t)sims[s].base + (dst[j] - (uint32_t)sims[s].coff);
+        if (dst[j] >= (uint32_t)n) {
+          raise_err(err, NB_DEVERR_SORT);
+          continue;
+        }
+      }
+      put[j] = true;
+    }
+    float4 pv[kSortBatch];
+    if (MODE != kSortMid) {
+#pragma unroll
+      for (int j = 0; j < kSortBatch; ++j)
+        if (put[j]) pv[j] = pos[vv[j]];
+    }
+#pragma unroll
+    for (int j = 0; j < kSortBatch; ++j) {
+      if (!put[j]) continue;
+      kout[dst[j]] = kk[j];
+      vout[dst[j]] = vv[j];
+      if (MODE != kSortMid) pos_sorted[dst[j]] = pv[j];
+    }
+  }
+}
+
+// Launches one sort pass with its staging buffer (dynamic shared memory).
+template <typename K, int MODE>
+static int launch_sort_pass(int tiles, cudaStream_t st, const K* kin, const uint32_t* vin,
+                            K* kout, uint32_t* vout, int n, int shift,
+                            const uint32_t* hist, uint32_t* status, uint32_t* ctr,
+                            unsigned* err, const float4* pos, float4* pos_sorted,
+                            const SimDesc* sims, int nsims) {
+  const int smem = kSortTile * (int)(sizeof(K) + sizeof(uint32_t));
+  NB_CUDA(cudaFuncSetAttribute(k_sort_pass<K, MODE>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_sort_pass<K, MODE><<<tiles, kSortThreads, smem, st>>>(
+      kin, vin, kout, vout, n, shift, hist, status, ctr, err, pos, pos_sorted, sims, nsims);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
 }
 
 template <typename K>
@@ -261,14 +367,13 @@ static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
     uint32_t* status = w.hist + 8 * kSortRadix + 8 + (size_t)p * w.status_tiles * kSortRadix;
     uint32_t* ctr = w.tile_ctr + p;
     if (p == passes - 1)
-      k_sort_pass<K, kSortLast><<<tiles, kSortThreads, 0, st>>>(
-          kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, a.pos,
-          w.pos_sorted, nullptr, 0);
+      NB_TRY((launch_sort_pass<K, kSortLast>(tiles, st, kin, vin, kalt, valt, a.n, 8 * p,
+                                             hist, status, ctr, w.err, a.pos,
+                                             w.pos_sorted, nullptr, 0)));
     else
-      k_sort_pass<K, kSortMid><<<tiles, kSortThreads, 0, st>>>(
-          kin, vin, kalt, valt, a.n, 8 * p, hist, status, ctr, w.err, nullptr,
-          nullptr, nullptr, 0);
-    NB_CUDA(cudaGetLastError());
+      NB_TRY((launch_sort_pass<K, kSortMid>(tiles, st, kin, vin, kalt, valt, a.n, 8 * p,
+                                            hist, status, ctr, w.err, nullptr, nullptr,
+                                            nullptr, 0)));
     K* tk = kin; kin = kalt; kalt = tk;
     uint32_t* tv = vin; vin = valt; valt = tv;
   }
@@ -785,7 +890,13 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
         c = leaf_cell(a.ps, lo);
       } else {   // a subtree finished below: its Karras id follows its direction
         const bool right = lo == 0 || (hi != ni && sm.delta[j + 1] > sm.delta[j]);
-        c = load_cell(a, right ? hi : lo);
+        const int kid = right ? hi : lo;
+        if (kid < ni) {
+          c = load_cell(a, kid);
+        } else {   // only after a failed sort (the whole tree as one item)
+          raise_err(a.err, NB_DEVERR_TREE);
+          c = leaf_cell(a.ps, lo);
+        }
       }
       push = finish_node(a, sm, run, j, j, lo, hi, -1, false, c);
     }
@@ -1029,14 +1140,13 @@ int launch_ens_sort(EnsArgs& e, cudaStream_t st) {
     uint32_t* status = e.status + (size_t)p * e.status_tiles * kSortRadix;
     uint32_t* ctr = e.tile_ctr + p;
     if (p == passes - 1)
-      k_sort_pass<uint64_t, kSortLastEnsemble><<<tiles, kSortThreads, 0, st>>>(
-          kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err, e.pos,
-          e.pos_sorted, e.sims, e.nsims);
+      NB_TRY((launch_sort_pass<uint64_t, kSortLastEnsemble>(
+          tiles, st, kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err,
+          e.pos, e.pos_sorted, e.sims, e.nsims)));
     else
-      k_sort_pass<uint64_t, kSortMid><<<tiles, kSortThreads, 0, st>>>(
-          kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err, nullptr,
-          nullptr, nullptr, 0);
-    NB_CUDA(cudaGetLastError());
+      NB_TRY((launch_sort_pass<uint64_t, kSortMid>(
+          tiles, st, kin, vin, kalt, valt, e.nslots, 8 * p, hist, status, ctr, e.err,
+          nullptr, nullptr, nullptr, 0)));
     uint64_t* tk = kin; kin = kalt; kalt = tk;
     uint32_t* tv = vin; vin = valt; valt = tv;
   }
