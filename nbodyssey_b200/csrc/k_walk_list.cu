@@ -61,6 +61,7 @@ struct ListSmem {
   unsigned emask[kLW][MASKED ? kList : 1];
   __align__(16) float amb[kLW][32 * 4];   // ambiguous nodes, pairs
   unsigned res[kLW][32];                  // their accept ballots
+  float4 ext[kLW][MASKED ? 1 : 6];        // targets of min / max x, y, z
 };
 
 // The walk of warp `wg` (targets 32wg .. 32wg+31 of the tree in `a`); all
@@ -82,6 +83,20 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
   const float lox = warp_min(bi.x), loy = warp_min(bi.y), loz = warp_min(bi.z);
   const float hix = warp_max(bi.x), hiy = warp_max(bi.y), hiz = warp_max(bi.z);
   const float theta2 = a.theta2;
+  if (!MASKED) {
+    // the targets at the group's extremes (warp semantics: one rejecting
+    // target opens a node for all)
+    const float lv[6] = {lox, hix, loy, hiy, loz, hiz};
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const float c = (e < 2) ? bi.x : (e < 4 ? bi.y : bi.z);
+      const int src = __ffs(__ballot_sync(full, c == lv[e])) - 1;
+      const float ex = __shfl_sync(full, bi.x, src), ey = __shfl_sync(full, bi.y, src),
+                  ez = __shfl_sync(full, bi.z, src);
+      if (lane == 0) sm.ext[w][e] = make_float4(ex, ey, ez, 0.f);
+    }
+  }
+  const float cmx = 0.5f * (lox + hix), cmy = 0.5f * (loy + hiy), cmz = 0.5f * (loz + hiz);
 
   const f2 nx = pk2(-bi.x, -bi.x), ny = pk2(-bi.y, -bi.y), nz = pk2(-bi.z, -bi.z);
   const f2 e2 = pk2(a.eps2, a.eps2);
@@ -182,9 +197,23 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
       const float fy = fmaxf(fabsf(cy - loy), fabsf(cy - hiy));
       const float fz = fmaxf(fabsf(cz - loz), fabsf(cz - hiz));
       const float dmax2 = fx * fx + fy * fy + fz * fz;
-      if (s2 < theta2 * dmin2 * 0.99999f) accm = M;
-      else if (s2 > theta2 * dmax2 * 1.00001f) accm = 0u;
-      else amb = true;
+      if (s2 < theta2 * dmin2 * 0.99999f) {
+        accm = M;
+      } else if (s2 > theta2 * dmax2 * 1.00001f) {
+        accm = 0u;
+      } else if (MASKED) {
+        amb = true;
+      } else {
+        // warp semantics: if the group's extreme target along the node's
+        // dominant direction rejects it (the exact per-target test), the
+        // node opens; otherwise it goes to the test of every target
+        const float rx = cx - cmx, ry = cy - cmy, rz = cz - cmz;
+        const float qx = fabsf(rx), qy = fabsf(ry), qz = fabsf(rz);
+        const int e = (qx >= qy && qx >= qz) ? (rx > 0.f ? 1 : 0)
+                                             : (qy >= qz ? (ry > 0.f ? 3 : 2) : (rz > 0.f ? 5 : 4));
+        const float4 q = sm.ext[w][e];
+        amb = accepts(s2, theta2, cx, cy, cz, q.x, q.y, q.z);
+      }
     }
     // nodes the box cannot settle: their owners stage them in shared memory
     // (pairs interleaved as (cx0,cx1,cy0,cy1)(cz0,cz1,s0,s1)); every lane
