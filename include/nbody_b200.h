@@ -45,6 +45,7 @@ extern "C" {
 #define NB_DEVERR_QUEUE 8u  /* a persistent work-queue wait hit its limit */
 #define NB_DEVERR_TREE 16u  /* the centre-of-mass climb met an inconsistent tree */
 #define NB_DEVERR_VISITS 32u /* a tree walk visited more nodes than the tree has */
+#define NB_DEVERR_BOUNDS 64u /* a tree-build write outside its tree (skipped) */
 
 /* ---- parameters (src/simulation.hpp:4-15: SimParams, ForceMethod,
  *      BhTraversal) ------------------------------------------------------- */

@@ -74,7 +74,6 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_TRY(dalloc(&w.pos_sorted, cap));
   NB_TRY(dalloc(&w.nodes, ni));
   NB_TRY(dalloc(&w.parent, 2 * (size_t)cap));
-  NB_TRY(dalloc(&w.visit, ni));
   for (int i = 0; i < 2; ++i) {
     NB_TRY(dalloc(&w.seg[i], build_seg_entries(cap)));
     NB_TRY(dalloc(&w.seg_count[i], build_seg_entries(cap)));
@@ -136,7 +135,7 @@ int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit) {
 
 void ws_free(Workspace& w) {
   cudaFree(w.keys); cudaFree(w.keys_alt); cudaFree(w.vals); cudaFree(w.vals_alt);
-  cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.parent); cudaFree(w.visit);
+  cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.parent);
   for (int i = 0; i < 2; ++i) { cudaFree(w.seg[i]); cudaFree(w.seg_count[i]); }
   cudaFree(w.sums); cudaFree(w.box_lo); cudaFree(w.box_hi); cudaFree(w.hist);
   cudaFree(w.bbox); cudaFree(w.bbox_part); cudaFree(w.bbox_ticket);
@@ -270,6 +269,7 @@ static int check_device_error(Workspace& w, cudaStream_t st) {
     if (e & NB_DEVERR_STACK) m += " (tree walk stack overflow)";
     if (e & NB_DEVERR_TREE) m += " (inconsistent tree in the centre-of-mass pass)";
     if (e & NB_DEVERR_VISITS) m += " (tree walk visit limit)";
+    if (e & NB_DEVERR_BOUNDS) m += " (tree-build write out of range, skipped)";
     if (e & NB_DEVERR_SORT) m += " (radix sort look-back wait limit)";
     if (e & NB_DEVERR_WAIT) m += " (bulk-copy barrier wait limit)";
     if (e & NB_DEVERR_QUEUE) m += " (work-queue wait limit)";

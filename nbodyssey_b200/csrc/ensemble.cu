@@ -24,6 +24,7 @@ struct nb_ensemble {
   EnsArgs e{};                 // device pointers as allocated
   SimDesc* d_sims = nullptr;
   int* d_blk = nullptr;
+  BuildPlan plan;              // tree-build levels (fixed membership)
   Workspace ews;               // energy scratch
   double* d_energy = nullptr;  // [nsims][6]
   bool primed = false;
@@ -85,8 +86,7 @@ int ens_enqueue(nb_ensemble* h, bool prime) {
   NB_TRY(launch_ens_prep(e, st));
   NB_TRY(launch_ens_morton(e, st));
   NB_TRY(launch_ens_sort(e, st));
-  NB_TRY(launch_ens_build(e, st));
-  NB_TRY(launch_ens_com(e, st));
+  NB_TRY(launch_ens_levels(e, h->plan, st));
   NB_TRY(launch_walk_list_ens(e, st));
   return NB_OK;
 }
@@ -199,7 +199,6 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if ((rc = ens_alloc(h, &e.perm_alt, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.nodes, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.parent, 2 * S)) != NB_OK) break;
-    if ((rc = ens_alloc(h, &e.visit, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.sums, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.box_lo, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.box_hi, S)) != NB_OK) break;
@@ -211,6 +210,18 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     e.tile_ctr = e.hist + 8 * kSortRadix;
     e.status = e.hist + 8 * kSortRadix + 8;
     if ((rc = ens_alloc(h, &e.err, 4)) != NB_OK) break;
+    if ((rc = plan_build(sims.data(), nsims, h->plan)) != NB_OK) break;
+    {
+      BuildRun* runs = nullptr;
+      if ((rc = ens_alloc(h, &runs, h->plan.runs.size())) != NB_OK) break;
+      e.runs = runs;
+      const size_t segs = plan_seg_entries(b, nsims);
+      for (int i = 0; i < 2; ++i) {
+        if ((rc = ens_alloc(h, &e.seg[i], segs)) != NB_OK) break;
+        if ((rc = ens_alloc(h, &e.seg_count[i], segs)) != NB_OK) break;
+      }
+      if (rc != NB_OK) break;
+    }
     if ((rc = ens_alloc(h, &h->d_energy, 6 * (size_t)nsims)) != NB_OK) break;
     cudaError_t ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess) { rc = set_error(NB_ERR_CUDA, cudaGetErrorString(ce)); break; }
@@ -232,6 +243,9 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(h->d_blk, blk.data(), sizeof(int) * blk.size(),
                            cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess && !h->plan.runs.empty())
+      ce = cudaMemcpyAsync((void*)e.runs, h->plan.runs.data(),
+                           sizeof(BuildRun) * h->plan.runs.size(), cudaMemcpyHostToDevice, st);
     size_t row = 0;
     for (int s = 0; s < nsims && ce == cudaSuccess; ++s) {
       ce = cudaMemcpyAsync(e.pos + h->base[s], pos4 + 4 * row, 16 * (size_t)n[s],

@@ -2,8 +2,8 @@
 //   Morton keys (+ the radix sort's digit histograms, fused)
 //   onesweep LSD radix sort (+ the position gather, fused into the last pass)
 //   Karras radix tree + bottom-up centres of mass / boxes / sizes (FP64
-//   mass-weighted sums): one fused bottom-up build in levels for a single
-//   tree, the top-down Karras build + climb for the trees of an ensemble.
+//   mass-weighted sums): one fused bottom-up build in levels, for a single
+//   tree or for all the trees of an ensemble at once.
 #include <cuda/atomic>
 
 #include "nb_internal.cuh"
@@ -390,164 +390,8 @@ int launch_sort(Workspace& w, const StepArgs& a, cudaStream_t st) {
   return sort_impl<uint32_t>(w, a, st);
 }
 
-// ---------------------------------------------------------------------------
-// Karras 2012 radix tree over the sorted keys (src/forces_bh.cu:234-277).
-// delta(i, j): common-prefix length, -1 outside [0, n); equal keys continue
-// with the sorted index (word bits + clz(i ^ j)).
-// ---------------------------------------------------------------------------
 __device__ __forceinline__ int clz_k(uint32_t x) { return __clz((int)x); }
 __device__ __forceinline__ int clz_k(uint64_t x) { return __clzll((long long)x); }
-
-template <typename K>
-__device__ __forceinline__ int delta_k(const K* __restrict__ keys, int n,
-                                       K ki, int i, int j) {
-  if (j < 0 || j >= n) return -1;
-  K x = ki ^ keys[j];
-  if (x) return clz_k(x);
-  return (int)(8 * sizeof(K)) + __clz(i ^ j);
-}
-
-// Internal node i of the tree over keys[0, n) (indices local to the tree).
-template <typename K>
-__device__ __forceinline__ void karras_node(const K* __restrict__ keys, int n,
-                                            int i, Node* nodes, int* parent,
-                                            int* visit) {
-  if (i == 0) parent[0] = -1;
-  if (i >= n - 1) return;
-  const K ki = keys[i];
-  int d = (delta_k(keys, n, ki, i, i + 1) - delta_k(keys, n, ki, i, i - 1)) >= 0
-              ? 1 : -1;
-  int dmin = delta_k(keys, n, ki, i, i - d);
-  int lmax = 2;
-  while (delta_k(keys, n, ki, i, i + lmax * d) > dmin) lmax <<= 1;
-  int l = 0;
-  for (int t = lmax >> 1; t > 0; t >>= 1)
-    if (delta_k(keys, n, ki, i, i + (l + t) * d) > dmin) l += t;
-  int j = i + l * d;
-  int first = min(i, j), last = max(i, j);
-  const K kf = keys[first];
-  int common = delta_k(keys, n, kf, first, last);
-  int split = first, step = last - first;
-  do {
-    step = (step + 1) >> 1;
-    if (split + step < last && delta_k(keys, n, kf, first, split + step) > common)
-      split += step;
-  } while (step > 1);
-  int left = (split == first) ? (n - 1 + split) : split;
-  int right = (split + 1 == last) ? (n - 1 + split + 1) : split + 1;
-  nodes[i].left = left;
-  nodes[i].right = right;
-  parent[left] = i;
-  parent[right] = i;
-  visit[i] = 0;
-}
-
-// ---------------------------------------------------------------------------
-// Bottom-up centres of mass over a built tree (src/forces_bh.cu:281-331),
-// used by the ensemble trees: every leaf climbs;
-// the first arrival at a node stops, the second combines both children
-// (left first, so the result does not depend on arrival order).  FP64
-// mass-weighted sums; node com = float(sum / mass); box = min/max of the
-// children's boxes; size2 = (longest edge)^2 in float.
-// ---------------------------------------------------------------------------
-// The climb from leaf i of the tree over ps[0, n) (indices local to the tree).
-__device__ __forceinline__ void com_climb(const float4* __restrict__ ps, int n,
-                                          int i, Node* nodes,
-                                          const int* __restrict__ parent,
-                                          int* visit, double4* sums,
-                                          float4* box_lo, float4* box_hi,
-                                          unsigned* err) {
-  if (i >= n) return;
-  const int ni = n - 1;
-  // the child this thread has finished: leaf i to begin with; its data stays
-  // in registers, only the sibling's is read after the arrival
-  int me = ni + i;
-  double s[2][4];
-  float l[2][3], h[2][3];
-  {
-    const float4 p = ps[i];
-    const double m = (double)p.w;
-    s[0][0] = __dmul_rn((double)p.x, m);
-    s[0][1] = __dmul_rn((double)p.y, m);
-    s[0][2] = __dmul_rn((double)p.z, m);
-    s[0][3] = m;
-    l[0][0] = h[0][0] = p.x;
-    l[0][1] = h[0][1] = p.y;
-    l[0][2] = h[0][2] = p.z;
-  }
-  int node = parent[me];
-  // a valid tree is at most n-1 levels deep; the bound and the range checks
-  // only matter if an earlier phase failed (its error word is then set)
-  for (int guard = 0; node >= 0; ++guard) {
-    if (node >= ni || guard >= n) {
-      raise_err(err, NB_DEVERR_TREE);
-      return;
-    }
-    // fetched before the arrival: the topology (from the build kernel) and a
-    // leaf sibling's position do not change during this kernel
-    const int2 ch = __ldcg(reinterpret_cast<const int2*>(&nodes[node].left));
-    const int up = __ldcg(&parent[node]);
-    if (ch.x < 0 || ch.y < 0 || ch.x >= 2 * n - 1 || ch.y >= 2 * n - 1 ||
-        (ch.x != me && ch.y != me)) {
-      raise_err(err, NB_DEVERR_TREE);
-      return;
-    }
-    const int sib = ch.x == me ? ch.y : ch.x;
-    float4 sp = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (sib >= ni) sp = ps[sib - ni];
-    // acq_rel: releases this thread's writes of the child it finished and
-    // acquires the sibling's, which the other arrival released
-    cuda::atomic_ref<int, cuda::thread_scope_device> arrivals(visit[node]);
-    if (arrivals.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
-    if (sib >= ni) {
-      const double m = (double)sp.w;
-      s[1][0] = __dmul_rn((double)sp.x, m);
-      s[1][1] = __dmul_rn((double)sp.y, m);
-      s[1][2] = __dmul_rn((double)sp.z, m);
-      s[1][3] = m;
-      l[1][0] = h[1][0] = sp.x;
-      l[1][1] = h[1][1] = sp.y;
-      l[1][2] = h[1][2] = sp.z;
-    } else {
-      const double2* qp = reinterpret_cast<const double2*>(&sums[sib]);
-      const double2 q0 = __ldcg(qp), q1 = __ldcg(qp + 1);
-      const float4 bl = __ldcg(&box_lo[sib]);
-      const float4 bh = __ldcg(&box_hi[sib]);
-      s[1][0] = q0.x; s[1][1] = q0.y; s[1][2] = q1.x; s[1][3] = q1.y;
-      l[1][0] = bl.x; l[1][1] = bl.y; l[1][2] = bl.z;
-      h[1][0] = bh.x; h[1][1] = bh.y; h[1][2] = bh.z;
-    }
-    // IEEE addition and min / max are commutative: which child is left does
-    // not change the bits
-    double4 q;
-    q.x = __dadd_rn(s[0][0], s[1][0]);
-    q.y = __dadd_rn(s[0][1], s[1][1]);
-    q.z = __dadd_rn(s[0][2], s[1][2]);
-    q.w = __dadd_rn(s[0][3], s[1][3]);
-    float4 com;
-    com.x = __double2float_rn(__ddiv_rn(q.x, q.w));
-    com.y = __double2float_rn(__ddiv_rn(q.y, q.w));
-    com.z = __double2float_rn(__ddiv_rn(q.z, q.w));
-    com.w = __double2float_rn(q.w);
-    float4 lo = make_float4(fminf(l[0][0], l[1][0]), fminf(l[0][1], l[1][1]),
-                            fminf(l[0][2], l[1][2]), 0.f);
-    float4 hi = make_float4(fmaxf(h[0][0], h[1][0]), fmaxf(h[0][1], h[1][1]),
-                            fmaxf(h[0][2], h[1][2]), 0.f);
-    float e = fmaxf(__fsub_rn(hi.x, lo.x),
-                    fmaxf(__fsub_rn(hi.y, lo.y), __fsub_rn(hi.z, lo.z)));
-    sums[node] = q;
-    box_lo[node] = lo;
-    box_hi[node] = hi;
-    nodes[node].com = com;
-    nodes[node].size2 = __fmul_rn(e, e);
-    // published by the release half of the next level's fetch_add
-    s[0][0] = q.x; s[0][1] = q.y; s[0][2] = q.z; s[0][3] = q.w;
-    l[0][0] = lo.x; l[0][1] = lo.y; l[0][2] = lo.z;
-    h[0][0] = hi.x; h[0][1] = hi.y; h[0][2] = hi.z;
-    me = node;
-    node = up;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Single-tree build: the Karras tree and its centres of mass, bottom up
@@ -614,6 +458,26 @@ struct LevelArgs {
   int seg;                          // segment capacity
   int fan;                          // segments per CTA
   unsigned* err;
+  // many trees (ensembles): one run per CTA, the arrays above then hold all
+  // simulations' slots and each run works on its simulation's slice
+  const BuildRun* runs;
+  const SimDesc* sims;
+};
+
+// The tree one CTA works on: the whole single tree, or one simulation's
+// slice of the ensemble arrays.  Built field by field in the kernel; the
+// kernel parameter itself is never modified.
+struct TreeView {
+  const LevelArgs& p;   // the kernel parameter (read in place)
+  int n;
+  int base;             // first slot of this tree in the arrays of p
+  __device__ const float4* ps() const { return p.ps + base; }
+  __device__ Node* nodes() const { return p.nodes + base; }
+  __device__ int* parent() const { return p.parent + 2 * (size_t)base; }
+  __device__ double4* sums() const { return p.sums + base; }
+  __device__ float4* box_lo() const { return p.box_lo + base; }
+  __device__ float4* box_hi() const { return p.box_hi + base; }
+  __device__ unsigned* err() const { return p.err; }
 };
 
 struct Cell {   // a finished node: FP64 mass-weighted sums and box
@@ -653,11 +517,15 @@ __device__ __forceinline__ Cell merge(const Cell& a, const Cell& b) {
 
 // Node record of internal node id over leaves [lo, hi] split after leaf sc,
 // and the parent links of its two children.
-__device__ __forceinline__ void write_node(const LevelArgs& a, int id, int lo,
+__device__ __forceinline__ void write_node(const TreeView& a, int id, int lo,
                                            int hi, int sc, const Cell& c) {
   const int ni = a.n - 1;
   const int l = sc == lo ? ni + sc : sc;
   const int r = sc + 1 == hi ? ni + sc + 1 : sc + 1;
+  if (id < 0 || id >= ni || l < 0 || r < 0 || l >= 2 * ni + 1 || r >= 2 * ni + 1) {
+    raise_err(a.err(), NB_DEVERR_BOUNDS);
+    return;
+  }
   float4 com;
   com.x = __double2float_rn(__ddiv_rn(c.s.x, c.s.w));
   com.y = __double2float_rn(__ddiv_rn(c.s.y, c.s.w));
@@ -665,26 +533,30 @@ __device__ __forceinline__ void write_node(const LevelArgs& a, int id, int lo,
   com.w = __double2float_rn(c.s.w);
   const float e = fmaxf(__fsub_rn(c.hi.x, c.lo.x),
                         fmaxf(__fsub_rn(c.hi.y, c.lo.y), __fsub_rn(c.hi.z, c.lo.z)));
-  float4* rec = reinterpret_cast<float4*>(&a.nodes[id]);
+  float4* rec = reinterpret_cast<float4*>(&a.nodes()[id]);
   rec[0] = com;
   reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(__fmul_rn(e, e)), 0);
-  a.parent[l] = id;
-  a.parent[r] = id;
+  a.parent()[l] = id;
+  a.parent()[r] = id;
 }
 
-__device__ __forceinline__ void store_cell(const LevelArgs& a, int id, const Cell& c) {
-  a.sums[id] = c.s;
-  a.box_lo[id] = c.lo;
-  a.box_hi[id] = c.hi;
+__device__ __forceinline__ void store_cell(const TreeView& a, int id, const Cell& c) {
+  if (id < 0 || id >= a.n - 1) {
+    raise_err(a.err(), NB_DEVERR_BOUNDS);
+    return;
+  }
+  a.sums()[id] = c.s;
+  a.box_lo()[id] = c.lo;
+  a.box_hi()[id] = c.hi;
 }
 
-__device__ __forceinline__ Cell load_cell(const LevelArgs& a, int id) {
+__device__ __forceinline__ Cell load_cell(const TreeView& a, int id) {
   Cell c;
-  const double2* q = reinterpret_cast<const double2*>(&a.sums[id]);
+  const double2* q = reinterpret_cast<const double2*>(&a.sums()[id]);
   const double2 q0 = __ldcg(q), q1 = __ldcg(q + 1);
   c.s = make_double4(q0.x, q0.y, q1.x, q1.y);
-  c.lo = __ldcg(&a.box_lo[id]);
-  c.hi = __ldcg(&a.box_hi[id]);
+  c.lo = __ldcg(&a.box_lo()[id]);
+  c.hi = __ldcg(&a.box_hi()[id]);
   return c;
 }
 
@@ -760,13 +632,13 @@ __device__ __forceinline__ void list_push(const LevelSmem& sm, int* count, int w
 // right, left end otherwise); an item and a node formed later share a slot
 // only when the item is below the node, and the node is written after the
 // item's cell was read.  Returns whether it parked.
-__device__ __forceinline__ bool finish_node(const LevelArgs& a, const LevelSmem& sm,
+__device__ __forceinline__ bool finish_node(const TreeView& a, const LevelSmem& sm,
                                             const Run& run, int ia, int ib, int lo,
                                             int hi, int sc, bool formed, const Cell& c) {
   const int ni = a.n - 1;
   if (lo == 0 && hi == ni) {   // the root: this run is the whole tree
     write_node(a, 0, lo, hi, sc, c);
-    a.parent[0] = -1;
+    a.parent()[0] = -1;
     return false;
   }
   const bool right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
@@ -788,7 +660,7 @@ __device__ __forceinline__ bool finish_node(const LevelArgs& a, const LevelSmem&
 // One pending arrival (items [ia, ib], parked in its slot) climbs until it
 // is the first at a split or finishes.  acq_rel: the exchange publishes this
 // thread's slot writes and acquires the sibling's.
-__device__ __forceinline__ void climb_arrival(const LevelArgs& a, const LevelSmem& sm,
+__device__ __forceinline__ void climb_arrival(const TreeView& a, const LevelSmem& sm,
                                               const Run& run, unsigned d) {
   const int ni = a.n - 1;
   int ia = (int)(d & 0xffffu), ib = (int)(d >> 16);
@@ -814,19 +686,40 @@ __device__ __forceinline__ void climb_arrival(const LevelArgs& a, const LevelSme
     if (!finish_node(a, sm, run, ia, ib, lo, hi, sm.pos[k], true, c)) return;
     right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
   }
-  raise_err(a.err, NB_DEVERR_TREE);
+  raise_err(a.err(), NB_DEVERR_TREE);
 }
 
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
+__global__ void __launch_bounds__(kLevelThreads, 2) k_build_level(LevelArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int C = FIRST ? kLeafGroup : kLevelItems;
   const LevelSmem sm(smem_raw, C);
-  const int n = a.n, ni = n - 1, g = blockIdx.x, tid = threadIdx.x;
+  // this CTA's tree, its group index there, its input segments [sfirst,
+  // sfirst + scount) and whether it hands open splits to the next level
+  const LevelArgs& p = args;
+  int tn = p.n, sbase = 0;
+  int g = blockIdx.x, sfirst = 0, scount = 0;
+  bool out = p.out_seg != nullptr;
+  if (p.runs) {
+    const BuildRun r = p.runs[blockIdx.x];
+    const SimDesc d = p.sims[r.sim];
+    if (!d.active || d.n < 2) return;
+    tn = d.n;
+    sbase = d.base;
+    g = r.group;
+    sfirst = r.in_first;
+    scount = r.in_count;
+    out = out && r.out;
+  } else if (!FIRST) {
+    sfirst = g * p.fan;
+    scount = min(p.fan, p.in_groups - sfirst);
+  }
+  const TreeView a{p, tn, sbase};
+  const int n = a.n, ni = n - 1, tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   Run run;
   if (FIRST) {
-    const K* __restrict__ keys = static_cast<const K*>(a.keys);
+    const K* __restrict__ keys = static_cast<const K*>(p.keys) + sbase;
     run.A = g * kLeafGroup;
     run.B = min(n, run.A + kLeafGroup);
     run.M = run.B < n ? run.B - run.A : run.B - run.A - 1;
@@ -836,9 +729,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
     }
     if (tid == 0) sm.delta[0] = run.A > 0 ? split_delta(keys, run.A - 1) : -1;
   } else {
-    const int r0 = g * a.fan, r1 = min(a.in_groups, r0 + a.fan);
+    const int r0 = sfirst, r1 = sfirst + scount;
     if (warp == 0) {   // segment offsets (fan <= 32)
-      const int c = r0 + lane < r1 ? min(a.in_count[r0 + lane], a.seg) : 0;
+      const int c = r0 + lane < r1 ? min(p.in_count[r0 + lane], p.seg) : 0;
       int incl = c;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -849,9 +742,9 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
       if (lane == 31) sm.scan[32] = incl;
       if (lane == 0) {   // the last entry below is the split left of this run
         int d = -1;
-        if (r0 > 0) {
-          const int cp = min(a.in_count[r0 - 1], a.seg);
-          if (cp > 0) d = a.in_seg[(size_t)(r0 - 1) * a.seg + cp - 1].y;
+        if (g > 0) {
+          const int cp = min(p.in_count[r0 - 1], p.seg);
+          if (cp > 0) d = p.in_seg[(size_t)(r0 - 1) * p.seg + cp - 1].y;
         }
         sm.delta[0] = d;
       }
@@ -863,13 +756,14 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
       const int off = sm.scan[r - r0];
       const int c = sm.scan[r - r0 + 1] - off;
       for (int e = lane; e < c; e += 32) {
-        const int2 v = a.in_seg[(size_t)r * a.seg + e];
+        const int2 v = p.in_seg[(size_t)r * p.seg + e];
         sm.pos[off + e] = v.x;
         sm.delta[off + e + 1] = v.y;
       }
     }
-    run.A = (int)min((long long)n, r0 * a.in_span);
-    run.B = (int)min((long long)n, r1 * a.in_span);
+    // region index of segment r within the tree: g * fan + (r - sfirst)
+    run.A = (int)min((long long)n, (long long)g * p.fan * p.in_span);
+    run.B = (int)min((long long)n, ((long long)g * p.fan + scount) * p.in_span);
   }
   run.items = run.B < n ? run.M : run.M + 1;
   run.local = run.B < n ? run.M - 1 : run.M;
@@ -887,15 +781,15 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
       const int lo = run.item_lo(sm, j), hi = run.item_hi(sm, j, ni);
       Cell c;
       if (FIRST || lo == hi) {
-        c = leaf_cell(a.ps, lo);
+        c = leaf_cell(a.ps(), lo);
       } else {   // a subtree finished below: its Karras id follows its direction
         const bool right = lo == 0 || (hi != ni && sm.delta[j + 1] > sm.delta[j]);
         const int kid = right ? hi : lo;
         if (kid < ni) {
           c = load_cell(a, kid);
         } else {   // only after a failed sort (the whole tree as one item)
-          raise_err(a.err, NB_DEVERR_TREE);
-          c = leaf_cell(a.ps, lo);
+          raise_err(a.err(), NB_DEVERR_TREE);
+          c = leaf_cell(a.ps(), lo);
         }
       }
       push = finish_node(a, sm, run, j, j, lo, hi, -1, false, c);
@@ -931,7 +825,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
         const int other = atomicExch(&sm.exch[k], right ? ia : ib);
         if (other != kSplitEmpty) {
           if (other < 0 || other >= run.items || (right ? other <= k : other > k)) {
-            raise_err(a.err, NB_DEVERR_TREE);
+            raise_err(a.err(), NB_DEVERR_TREE);
           } else {
             const Cell mine = get_cell(sm, right ? ib : ia);
             const Cell o = get_cell(sm, right ? k + 1 : k);
@@ -959,7 +853,7 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
     const int4 m = sm.meta[j];
     if (m.w >= 0) write_node(a, m.w, m.x, m.y, m.z, get_cell(sm, j));
   }
-  if (!a.out_seg) return;
+  if (!out) return;
   // a formed child waiting at an open split hands its cell to the next level
   for (int k = tid; k < run.local; k += kLevelThreads) {
     const int e = sm.exch[k];
@@ -991,13 +885,14 @@ __global__ void __launch_bounds__(kLevelThreads) k_build_level(LevelArgs a) {
   int off = base + incl - cnt;
   for (int k = k0; k < k1; ++k) {
     if (k >= run.local || sm.exch[k] != kSplitDone) {
-      if (off < a.seg) a.out_seg[(size_t)g * a.seg + off] = make_int2(sm.pos[k], sm.delta[k + 1]);
+      if (off < p.seg)
+        p.out_seg[(size_t)blockIdx.x * p.seg + off] = make_int2(sm.pos[k], sm.delta[k + 1]);
       ++off;
     }
   }
   if (tid == 0) {
-    a.out_count[g] = min(total, a.seg);
-    if (total > a.seg) raise_err(a.err, NB_DEVERR_TREE);
+    p.out_count[blockIdx.x] = min(total, p.seg);
+    if (total > p.seg) raise_err(a.err(), NB_DEVERR_TREE);
   }
 }
 
@@ -1157,40 +1052,95 @@ int launch_ens_sort(EnsArgs& e, cudaStream_t st) {
   return NB_OK;
 }
 
-__global__ void __launch_bounds__(256) k_ens_karras(EnsArgs e) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= e.nslots) return;
-  const int s = e.blk_sim[g >> 5];
-  if (s < 0) return;
-  const SimDesc d = e.sims[s];
-  if (!d.active || d.n < 2) return;
-  karras_node<uint64_t>(e.keys + d.base, d.n, g - d.base, e.nodes + d.base,
-                        e.parent + 2 * d.base, e.visit + d.base);
-}
-
-__global__ void __launch_bounds__(256) k_ens_com(EnsArgs e) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= e.nslots) return;
-  const int s = e.blk_sim[g >> 5];
-  if (s < 0) return;
-  const SimDesc d = e.sims[s];
-  if (!d.active || d.n < 2) return;
-  com_climb(e.pos_sorted + d.base, d.n, g - d.base, e.nodes + d.base,
-            e.parent + 2 * d.base, e.visit + d.base, e.sums + d.base,
-            e.box_lo + d.base, e.box_hi + d.base, e.err);
-}
-
-int launch_ens_build(const EnsArgs& e, cudaStream_t st) {
-  const int blocks = (e.nslots + 255) / 256;
-  k_ens_karras<<<blocks, 256, 0, st>>>(e);
-  NB_CUDA(cudaGetLastError());
+// Ensemble trees: the level kernels over a plan of runs.  Level 1 has one
+// run per (simulation, 1024-leaf group); a simulation with G groups at one
+// level has ceil(G / fan) runs at the next, each over fan consecutive
+// segments of its own runs below; a simulation is done at the level where it
+// has one run.  The 64-bit keys (sim << 30) | morton30 give the same
+// Cartesian tree as the simulation's own keys (the shared prefix shifts every
+// d by 32), so each tree equals the one the simulation builds alone.
+int plan_build(const SimDesc* sims, int nsims, BuildPlan& plan) {
+  plan.levels = 0;
+  plan.runs.clear();
+  std::vector<int> groups(nsims, 0), first(nsims, 0);
+  int live = 0;
+  for (int s = 0; s < nsims; ++s)
+    if (sims[s].active && sims[s].n >= 2) {
+      groups[s] = (sims[s].n + kLeafGroup - 1) / kLeafGroup;
+      ++live;
+    }
+  if (!live) return NB_OK;
+  const int fan = level_fan(30);
+  for (int lv = 0;; ++lv) {
+    if (lv >= kBuildMaxLevels) return set_error(NB_ERR_INVALID, "build plan too deep");
+    plan.offset[lv] = (int)plan.runs.size();
+    bool more = false;
+    for (int s = 0; s < nsims; ++s) {
+      const int G = groups[s];
+      if (G == 0 || (lv > 0 && G == 1)) continue;
+      const int next_first = (int)plan.runs.size();
+      if (lv == 0) {
+        for (int g = 0; g < G; ++g) plan.runs.push_back({s, g, 0, 0, G > 1 ? 1 : 0});
+      } else {
+        const int Gn = (G + fan - 1) / fan;
+        for (int g = 0; g < Gn; ++g)
+          plan.runs.push_back({s, g, first[s] + g * fan, std::min(fan, G - g * fan),
+                               Gn > 1 ? 1 : 0});
+        groups[s] = Gn;
+      }
+      first[s] = next_first - plan.offset[lv];   // index within this level
+      if (groups[s] > 1) more = true;
+    }
+    plan.count[lv] = (int)plan.runs.size() - plan.offset[lv];
+    plan.levels = lv + 1;
+    if (!more) break;
+  }
   return NB_OK;
 }
 
-int launch_ens_com(const EnsArgs& e, cudaStream_t st) {
-  const int blocks = (e.nslots + 255) / 256;
-  k_ens_com<<<blocks, 256, 0, st>>>(e);
-  NB_CUDA(cudaGetLastError());
+size_t plan_seg_entries(int slots, int nsims) {
+  return ((size_t)slots / kLeafGroup + (size_t)nsims + 1) * level_seg(30);
+}
+
+int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st) {
+  LevelArgs b{};
+  b.keys = e.keys;
+  b.ps = e.pos_sorted;
+  b.nodes = e.nodes;
+  b.parent = e.parent;
+  b.sums = e.sums;
+  b.box_lo = e.box_lo;
+  b.box_hi = e.box_hi;
+  b.seg = level_seg(30);
+  b.fan = level_fan(30);
+  b.err = e.err;
+  b.sims = e.sims;
+  long long span = kLeafGroup;
+  for (int lv = 0; lv < plan.levels; ++lv) {
+    const int runs = plan.count[lv];
+    if (runs == 0) continue;
+    b.runs = e.runs + plan.offset[lv];
+    if (lv > 0) {
+      b.in_seg = e.seg[(lv - 1) & 1];
+      b.in_count = e.seg_count[(lv - 1) & 1];
+      b.in_span = span;
+      span *= b.fan;
+    }
+    b.out_seg = lv + 1 < plan.levels ? e.seg[lv & 1] : nullptr;
+    b.out_count = lv + 1 < plan.levels ? e.seg_count[lv & 1] : nullptr;
+    if (lv == 0) {
+      const int smem = (int)level_smem(kLeafGroup);
+      NB_CUDA(cudaFuncSetAttribute(k_build_level<uint64_t, true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      k_build_level<uint64_t, true><<<runs, kLevelThreads, smem, st>>>(b);
+    } else {
+      const int smem = (int)level_smem(kLevelItems);
+      NB_CUDA(cudaFuncSetAttribute(k_build_level<uint32_t, false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      k_build_level<uint32_t, false><<<runs, kLevelThreads, smem, st>>>(b);
+    }
+    NB_CUDA(cudaGetLastError());
+  }
   return NB_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/nbody_b200.h"
 
@@ -75,7 +76,6 @@ struct Workspace {
   float4* pos_sorted = nullptr;   // [cap]
   Node* nodes = nullptr;          // [cap-1]
   int* parent = nullptr;          // [2cap-1]
-  int* visit = nullptr;           // [cap-1]
   int2* seg[2] = {nullptr, nullptr};      // open splits per build CTA,
   int* seg_count[2] = {nullptr, nullptr}; // ping-pong between levels
   double4* sums = nullptr;        // [cap-1] FP64 mass-weighted sums
@@ -196,6 +196,25 @@ constexpr int kEnsSimBits = 10;                     // sim id field of the keys
 constexpr int kEnsMaxSims = (1 << kEnsSimBits) - 1; // id 1023 marks unused slots
 constexpr int kEnsKeyBits = 30 + kEnsSimBits;       // 40 bits, 5 sort passes
 
+// One CTA of a multi-tree build level.
+struct BuildRun {
+  int sim;        // simulation (index into the SimDesc table)
+  int group;      // its group at this level
+  int in_first;   // first segment of the level below (later levels)
+  int in_count;   // segments it merges
+  int out;        // 1: hands its open splits to the next level
+};
+
+constexpr int kBuildMaxLevels = 8;
+
+// Host plan: the runs of every level back to back.
+struct BuildPlan {
+  int levels = 0;
+  int offset[kBuildMaxLevels] = {};
+  int count[kBuildMaxLevels] = {};
+  std::vector<BuildRun> runs;
+};
+
 struct EnsArgs {
   int nsims;
   int nslots;                 // slot extent (multiple of 32)
@@ -213,7 +232,6 @@ struct EnsArgs {
   uint32_t* perm_alt;
   Node* nodes;                // [nslots]
   int* parent;                // [2 nslots]
-  int* visit;                 // [nslots]
   double4* sums;              // [nslots]
   float4* box_lo;
   float4* box_hi;
@@ -226,13 +244,19 @@ struct EnsArgs {
   unsigned* err;
   bool kick_drift;
   bool kick_after;
+  const BuildRun* runs;       // tree-build plan (all levels)
+  int2* seg[2];               // open splits between build levels
+  int* seg_count[2];
 };
 
 int launch_ens_prep(const EnsArgs& e, cudaStream_t st);
 int launch_ens_morton(const EnsArgs& e, cudaStream_t st);
 int launch_ens_sort(EnsArgs& e, cudaStream_t st);   // updates e.keys / e.perm
-int launch_ens_build(const EnsArgs& e, cudaStream_t st);
-int launch_ens_com(const EnsArgs& e, cudaStream_t st);
+// Tree build of all simulations (k_lbvh.cu): a host plan of level runs,
+// uploaded to e.runs, then one launch per level.
+int plan_build(const SimDesc* sims, int nsims, BuildPlan& plan);
+size_t plan_seg_entries(int slots, int nsims);
+int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st);
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
 
 // A view of a simulation handle's device state (defined in api.cu) for the

@@ -36,8 +36,9 @@ using namespace nb;
 namespace {
 
 constexpr size_t kBytesPerSlot = 224;   // state 64, sorted 16, keys 16, perm 8,
-                                        // nodes 32, parent 8, visit 4, sums 32,
-                                        // boxes 32, sort scratch ~12
+                                        // nodes 32, parent 8, sums 32, boxes 32,
+                                        // sort scratch ~12, build plan and
+                                        // segments ~4
 constexpr int kInFlight = 2;            // engine steps queued ahead of the GPU
 constexpr int kFrameSlots = 8;
 
@@ -87,6 +88,8 @@ struct nb_server {
   std::map<int, int> free_blocks;    // start block -> length (32-slot blocks)
   std::vector<int> free_ids;
   bool table_dirty = false;
+  BuildPlan plan;                    // tree-build levels of the running sims
+  size_t plan_cap = 0;               // BuildRun entries allocated at e.runs
   cudaStream_t stream = nullptr, side = nullptr;
   cudaEvent_t step_ev[kInFlight] = {};
   long long step_count = 0;
@@ -298,6 +301,13 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
                             cudaMemcpyHostToDevice, s->stream));
     NB_CUDA(cudaMemcpyAsync((void*)s->e.blk_sim, s->blk.data(), sizeof(int) * (extent / 32),
                             cudaMemcpyHostToDevice, s->stream));
+    NB_TRY(plan_build(s->sims.data(), nsims, s->plan));
+    if (s->plan.runs.size() > s->plan_cap)
+      return set_error(NB_ERR_INVALID, "tree-build plan exceeds its buffer");
+    if (!s->plan.runs.empty())
+      NB_CUDA(cudaMemcpyAsync((void*)s->e.runs, s->plan.runs.data(),
+                              sizeof(BuildRun) * s->plan.runs.size(),
+                              cudaMemcpyHostToDevice, s->stream));
     s->table_dirty = false;
   }
   // bound the queue depth: wait for the step issued kInFlight iterations ago
@@ -318,8 +328,7 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
   NB_TRY(launch_ens_prep(e, s->stream));
   NB_TRY(launch_ens_morton(e, s->stream));
   NB_TRY(launch_ens_sort(e, s->stream));
-  NB_TRY(launch_ens_build(e, s->stream));
-  NB_TRY(launch_ens_com(e, s->stream));
+  NB_TRY(launch_ens_levels(e, s->plan, s->stream));
   NB_TRY(launch_walk_list_ens(e, s->stream));
   NB_CUDA(cudaEventRecord(ev, s->stream));
   s->step_count += 1;
@@ -429,7 +438,6 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     if ((rc = srv_alloc(s, &e.perm_alt, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.nodes, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.parent, 2 * S)) != NB_OK) break;
-    if ((rc = srv_alloc(s, &e.visit, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.sums, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.box_lo, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.box_hi, S)) != NB_OK) break;
@@ -441,6 +449,22 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     e.tile_ctr = e.hist + 8 * kSortRadix;
     e.status = e.hist + 8 * kSortRadix + 8;
     if ((rc = srv_alloc(s, &e.err, 4)) != NB_OK) break;
+    {
+      // a simulation with G > 1 groups of 1024 leaves has G runs at the
+      // first level and at most G / 15 + 1 at each later one: at most three
+      // runs per 1024 of its slots (G = 2 is the worst); one with G = 1 has
+      // one run
+      s->plan_cap = 3 * (S / 1024 + 1) + 2 * (size_t)max_sims + 64;
+      BuildRun* runs = nullptr;
+      if ((rc = srv_alloc(s, &runs, s->plan_cap)) != NB_OK) break;
+      e.runs = runs;
+      const size_t segs = plan_seg_entries((int)S, max_sims);
+      for (int i = 0; i < 2; ++i) {
+        if ((rc = srv_alloc(s, &e.seg[i], segs)) != NB_OK) break;
+        if ((rc = srv_alloc(s, &e.seg_count[i], segs)) != NB_OK) break;
+      }
+      if (rc != NB_OK) break;
+    }
     s->frame_cap = std::min<int>((int)S, 1 << 21);
     if ((rc = srv_alloc(s, &s->d_frame, (size_t)kFrameSlots * s->frame_cap)) != NB_OK) break;
     cudaError_t ce = cudaMallocHost((void**)&s->h_frame, 16 * (size_t)kFrameSlots * s->frame_cap);
