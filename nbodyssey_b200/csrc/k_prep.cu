@@ -193,60 +193,85 @@ int launch_prep(Workspace& w, const StepArgs& s, bool bbox, bool pack,
 }
 
 // Ensemble prep: kick + drift of every live slot, each simulation's bounding
-// box (warp min/max, then one atomic per component and warp; warps never mix
-// simulations), and zeroing of the sort scratch.  The boxes must hold the
-// empty sentinels on entry (launch_ens_prep sets them).
+// box, and zeroing of the sort scratch.  Each warp takes a contiguous run of
+// 32-slot blocks (a block never mixes simulations) and keeps per-lane
+// min / max while the simulation stays the same; at a change of simulation
+// and at the end it reduces over the warp and issues one atomic per
+// component.  The boxes must hold the empty sentinels on entry
+// (launch_ens_prep sets them).
+__device__ __forceinline__ void ens_box_flush(const EnsArgs& e, int s, int* r) {
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    r[c] = __reduce_min_sync(0xffffffffu, r[c]);
+    r[c + 3] = __reduce_max_sync(0xffffffffu, r[c + 3]);
+  }
+  if ((threadIdx.x & 31) == 0 && s >= 0) {
+    for (int c = 0; c < 3; ++c) {
+      if (r[c] != 0x7fffffff) atomicMin(&e.bbox_min[4 * s + c], r[c]);
+      if (r[c + 3] != (int)0x80000000) atomicMax(&e.bbox_max[4 * s + c], r[c + 3]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    r[c] = 0x7fffffff;
+    r[c + 3] = (int)0x80000000;
+  }
+}
+
 template <bool KD>
 __global__ void __launch_bounds__(kPrepThreads) k_ens_prep(EnsArgs e,
                                                            uint32_t* zero,
                                                            int zero_words) {
-  const int stride = gridDim.x * blockDim.x;   // a multiple of 32
-  for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < e.nslots;
-       slot += stride) {
-    const int s = e.blk_sim[slot >> 5];         // the same for the whole warp
-    if (s < 0) continue;
-    const SimDesc d = e.sims[s];
-    const bool valid = d.active && slot - d.base < d.n;
-    int r[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000,
-                (int)0x80000000, (int)0x80000000};
-    if (valid) {
-      float4 x = e.pos[slot];
-      if (KD && d.active == 1) {
-        float4 v = e.vel[slot];
-        const float4 ac = e.acc[slot];
-        v.x = __fmaf_rn(d.half_dt, ac.x, v.x);
-        v.y = __fmaf_rn(d.half_dt, ac.y, v.y);
-        v.z = __fmaf_rn(d.half_dt, ac.z, v.z);
-        e.vel[slot] = v;
-        if (d.compensated) {
-          float4 l = e.pos_lo[slot];
-          drift_comp(x.x, l.x, v.x, d.dt);
-          drift_comp(x.y, l.y, v.y, d.dt);
-          drift_comp(x.z, l.z, v.z, d.dt);
-          e.pos_lo[slot] = l;
-        } else {
-          x.x = __fmaf_rn(d.dt, v.x, x.x);
-          x.y = __fmaf_rn(d.dt, v.y, x.y);
-          x.z = __fmaf_rn(d.dt, v.z, x.z);
-        }
-        e.pos[slot] = x;
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nblk = e.nslots >> 5;
+  const int per = (nblk + warps - 1) / warps;
+  const int b0 = min(nblk, wid * per), b1 = min(nblk, b0 + per);
+  int r[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, (int)0x80000000,
+              (int)0x80000000, (int)0x80000000};
+  int cur = -1;
+  SimDesc d{};
+  for (int b = b0; b < b1; ++b) {
+    const int s = e.blk_sim[b];                 // the same for the whole warp
+    if (s != cur) {
+      ens_box_flush(e, cur, r);
+      cur = s;
+      if (s >= 0) d = e.sims[s];
+    }
+    if (s < 0 || !d.active) continue;
+    const int slot = b * 32 + lane;
+    if (slot - d.base >= d.n) continue;
+    float4 x = e.pos[slot];
+    if (KD && d.active == 1) {
+      float4 v = e.vel[slot];
+      const float4 ac = e.acc[slot];
+      v.x = __fmaf_rn(d.half_dt, ac.x, v.x);
+      v.y = __fmaf_rn(d.half_dt, ac.y, v.y);
+      v.z = __fmaf_rn(d.half_dt, ac.z, v.z);
+      e.vel[slot] = v;
+      if (d.compensated) {
+        float4 l = e.pos_lo[slot];
+        drift_comp(x.x, l.x, v.x, d.dt);
+        drift_comp(x.y, l.y, v.y, d.dt);
+        drift_comp(x.z, l.z, v.z, d.dt);
+        e.pos_lo[slot] = l;
+      } else {
+        x.x = __fmaf_rn(d.dt, v.x, x.x);
+        x.y = __fmaf_rn(d.dt, v.y, x.y);
+        x.z = __fmaf_rn(d.dt, v.z, x.z);
       }
-      r[0] = r[3] = f2ord(x.x);
-      r[1] = r[4] = f2ord(x.y);
-      r[2] = r[5] = f2ord(x.z);
+      e.pos[slot] = x;
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      r[c] = __reduce_min_sync(0xffffffffu, r[c]);
-      r[c + 3] = __reduce_max_sync(0xffffffffu, r[c + 3]);
-    }
-    if ((threadIdx.x & 31) == 0 && d.active) {
-      for (int c = 0; c < 3; ++c) {
-        atomicMin(&e.bbox_min[4 * s + c], r[c]);
-        atomicMax(&e.bbox_max[4 * s + c], r[c + 3]);
-      }
-    }
+    r[0] = min(r[0], f2ord(x.x));
+    r[1] = min(r[1], f2ord(x.y));
+    r[2] = min(r[2], f2ord(x.z));
+    r[3] = max(r[3], f2ord(x.x));
+    r[4] = max(r[4], f2ord(x.y));
+    r[5] = max(r[5], f2ord(x.z));
   }
+  ens_box_flush(e, (cur >= 0 && d.active) ? cur : -1, r);
+  const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < zero_words; i += stride)
     zero[i] = 0u;
 }
