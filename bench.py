@@ -361,23 +361,22 @@ def run_b200(args, rank, world, local, pg):
     graph_ms = sim.elapsed_ms(0, 1)
     clk = clocks.stop() or clk
 
-    # end to end: pinned host state in, step, state out, every step
+    # end to end: pinned host state in, one step, state out, every step
+    # (nb_step_host; each step's inputs are the previous step's outputs)
     keep = []
-    hp = pinned_array(lib, (n, 4), keep)
-    hv = pinned_array(lib, (n, 4), keep)
-    ha = pinned_array(lib, (n, 4), keep)
-    L.check(lib.nb_get_positions(sim._h, L.ptr(hp)))
-    L.check(lib.nb_get_velocities(sim._h, L.ptr(hv)))
-    L.check(lib.nb_get_accelerations(sim._h, L.ptr(ha)))
+    bufs = [[pinned_array(lib, (n, 4), keep) for _ in range(3)] for _ in range(2)]
+    L.check(lib.nb_get_positions(sim._h, L.ptr(bufs[0][0])))
+    L.check(lib.nb_get_velocities(sim._h, L.ptr(bufs[0][1])))
+    L.check(lib.nb_get_accelerations(sim._h, L.ptr(bufs[0][2])))
+    cur = 0
     for it in range(args.e2e_steps + 2):
         if it == 2:
             dist_barrier(pg)
             t0 = time.perf_counter()
-        L.check(lib.nb_set_state_acc(sim._h, L.ptr(hp), L.ptr(hv), L.ptr(ha)))
-        L.check(lib.nb_step(sim._h, 1))
-        L.check(lib.nb_get_positions(sim._h, L.ptr(hp)))
-        L.check(lib.nb_get_velocities(sim._h, L.ptr(hv)))
-        L.check(lib.nb_get_accelerations(sim._h, L.ptr(ha)))
+        i, o = bufs[cur], bufs[cur ^ 1]
+        L.check(lib.nb_step_host(sim._h, L.ptr(i[0]), L.ptr(i[1]), L.ptr(i[2]),
+                                 L.ptr(o[0]), L.ptr(o[1]), L.ptr(o[2])))
+        cur ^= 1
     e2e_s = dist_max(pg, time.perf_counter() - t0)
     for p in keep:
         lib.nb_free_pinned(p)
@@ -411,8 +410,9 @@ def run_b200(args, rank, world, local, pg):
                         * args.steps,
         "e2e": {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
-                "path": "nb_set_state_acc + nb_step + nb_get_{positions,"
-                        "velocities,accelerations}, pinned host buffers, wall clock"},
+                "path": "nb_step_host: pinned host pos / vel / a(x) in, one step, "
+                        "pos / vel / a(x_new) out (positions return on a second "
+                        "stream during the tree build and walk), wall clock"},
         "roofline": {"kernel": (("k_walk_list" if args.walk == "list" else "k_walk_%s" % args.traverse) if args.force == "bh"
                                 else "k_allpairs"), "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",

@@ -122,6 +122,16 @@ NB_API int nb_get_accelerations(nb_sim* s, float* acc4);
  * force evaluation (a host round trip of pos / vel / acc between steps). */
 NB_API int nb_set_state_acc(nb_sim* s, const float* pos4, const float* vel4,
                             const float* acc4);
+/* leapfrog_step (src/integrator.cuh:19) on host-resident state, for callers
+ * that keep the state in host memory between steps: uploads pos / vel and
+ * a(x), steps once, and writes the new pos / vel / a(x_new) to the out
+ * buffers.  The positions are final after the drift and return to the host
+ * on a second stream while the tree is built and walked.  Synchronous;
+ * pinned host buffers (nb_alloc_pinned) give full PCIe speed.  Same results
+ * as nb_set_state_acc + nb_step(1) + the three downloads. */
+NB_API int nb_step_host(nb_sim* s, const float* pos4, const float* vel4,
+                        const float* acc4, float* pos_out4, float* vel_out4,
+                        float* acc_out4);
 
 /* compute_forces (src/forces.cuh:8, src/forces.cu:68-86): a(x) for the
  * current positions into the simulation's acceleration buffer, in original

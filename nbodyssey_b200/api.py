@@ -140,6 +140,21 @@ class Simulation:
     def velocities(self):
         return self._get(self._lib.nb_get_velocities)
 
+    def accelerations(self):
+        """The acceleration buffer: a(x) of the current positions after a
+        step or compute_forces."""
+        return self._get(self._lib.nb_get_accelerations)
+
+    def set_state_acc(self, pos4, vel4, acc4):
+        """Uploads a state with its a(x): the next step needs no priming
+        force evaluation."""
+        pos4 = _rows4(pos4, "pos4")
+        vel4 = _rows4(vel4, "vel4")
+        acc4 = _rows4(acc4, "acc4")
+        if not (pos4.shape == vel4.shape == acc4.shape) or pos4.shape[0] != self.n:
+            raise ValueError("pos4 / vel4 / acc4 must be (n, 4)")
+        L.check(self._lib.nb_set_state_acc(self._h, L.ptr(pos4), L.ptr(vel4), L.ptr(acc4)))
+
     def position_lo(self):
         return self._get(self._lib.nb_get_position_lo)
 
@@ -147,6 +162,19 @@ class Simulation:
     def compute_forces(self):
         """compute_forces (src/forces.cu:68-86): a(x), original order."""
         return self._get(self._lib.nb_compute_forces)
+
+    def step_host(self, pos4, vel4, acc4, out=None):
+        """One leapfrog step of host-resident state: (pos, vel, a(x)) in,
+        (pos, vel, a(x_new)) out (nb_step_host).  `out` may give the three
+        output arrays (pinned ones avoid a staging copy)."""
+        pos4 = _rows4(pos4, "pos4")
+        vel4 = _rows4(vel4, "vel4")
+        acc4 = _rows4(acc4, "acc4")
+        if out is None:
+            out = tuple(np.empty_like(pos4) for _ in range(3))
+        L.check(self._lib.nb_step_host(self._h, L.ptr(pos4), L.ptr(vel4), L.ptr(acc4),
+                                       L.ptr(out[0]), L.ptr(out[1]), L.ptr(out[2])))
+        return out
 
     def step(self, nsteps=1):
         """leapfrog_step x nsteps (asynchronous; see sync())."""

@@ -197,6 +197,7 @@ static StepArgs make_args(int n, float4* pos, float4* lo, float4* vel,
   a.t0 = 0;
   a.t1 = n;
   a.part = nullptr;
+  a.after_prep = nullptr;
   return a;
 }
 
@@ -229,18 +230,21 @@ static int enqueue_forces(Workspace& w, const StepArgs& a, int force,
   if (pm) NB_CUDA(cudaEventRecord(pm->start, st));
   if (force == NB_FORCE_BH && a.n < 2) {
     if (a.kick_drift) NB_TRY(launch_prep(w, a, false, false, st));
+    if (a.after_prep) NB_CUDA(cudaEventRecord(a.after_prep, st));
     NB_CUDA(cudaMemsetAsync(a.acc, 0, sizeof(float4) * a.n, st));
     return mark(pm, NB_PHASE_WALK, st);
   }
   if (force == NB_FORCE_NAIVE) {
     NB_TRY(ws_reserve_allpairs(w, a.n, allpairs_geometry(a.n).jsplit));
     NB_TRY(launch_prep(w, a, false, true, st));
+    if (a.after_prep) NB_CUDA(cudaEventRecord(a.after_prep, st));
     NB_TRY(mark(pm, NB_PHASE_PREP, st));
     NB_TRY(launch_allpairs(w, a, st));
     return mark(pm, NB_PHASE_WALK, st);
   }
   NB_TRY(ws_reserve(w, a.n, a.key_bits));
   NB_TRY(launch_prep(w, a, true, false, st));
+  if (a.after_prep) NB_CUDA(cudaEventRecord(a.after_prep, st));
   NB_TRY(mark(pm, NB_PHASE_PREP, st));
   NB_TRY(launch_morton(w, a, st));
   NB_TRY(mark(pm, NB_PHASE_MORTON, st));
@@ -310,6 +314,9 @@ struct nb_sim {
   cudaEvent_t slots[16] = {};
   void* flush_buf = nullptr;
   size_t flush_bytes = 0;
+  // nb_step_host: positions leave on a side stream once the drift is done
+  cudaStream_t io_stream = nullptr;
+  cudaEvent_t io_prep = nullptr;
 };
 
 static void sim_free(nb_sim* s) {
@@ -324,6 +331,11 @@ static void sim_free(nb_sim* s) {
   }
   for (auto& e : s->slots)
     if (e) cudaEventDestroy(e);
+  if (s->io_stream) {
+    cudaStreamSynchronize(s->io_stream);
+    cudaStreamDestroy(s->io_stream);
+  }
+  if (s->io_prep) cudaEventDestroy(s->io_prep);
   cudaFree(s->flush_buf);
   cudaFree(s->pos);
   cudaFree(s->pos_lo);
@@ -608,6 +620,31 @@ int nb_get_accelerations(nb_sim* s, float* acc4) { return download(s, acc4, s ? 
 int nb_get_positions(nb_sim* s, float* pos4) { return download(s, pos4, s ? s->pos : nullptr); }
 int nb_get_velocities(nb_sim* s, float* vel4) { return download(s, vel4, s ? s->vel : nullptr); }
 int nb_get_position_lo(nb_sim* s, float* lo4) { return download(s, lo4, s ? s->pos_lo : nullptr); }
+
+int nb_step_host(nb_sim* s, const float* pos4, const float* vel4, const float* acc4,
+                 float* pos_out4, float* vel_out4, float* acc_out4) {
+  if (!s || !pos4 || !vel4 || !acc4 || !pos_out4 || !vel_out4 || !acc_out4)
+    return set_error(NB_ERR_INVALID, "NULL argument");
+  if (!s->io_stream)
+    NB_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking));
+  if (!s->io_prep) NB_CUDA(cudaEventCreateWithFlags(&s->io_prep, cudaEventDisableTiming));
+  NB_TRY(nb_set_state_acc(s, pos4, vel4, acc4));
+  const size_t b = sizeof(float4) * s->n;
+  StepArgs a = sim_args(s);
+  a.kick_drift = true;
+  a.kick_after = true;
+  a.after_prep = s->io_prep;
+  NB_TRY(enqueue_forces(s->ws, a, s->p.force, s->stream, nullptr));
+  // positions are final after the drift: they cross PCIe while the tree is
+  // built and walked
+  NB_CUDA(cudaStreamWaitEvent(s->io_stream, s->io_prep, 0));
+  NB_CUDA(cudaMemcpyAsync(pos_out4, s->pos, b, cudaMemcpyDeviceToHost, s->io_stream));
+  NB_CUDA(cudaMemcpyAsync(vel_out4, s->vel, b, cudaMemcpyDeviceToHost, s->stream));
+  NB_CUDA(cudaMemcpyAsync(acc_out4, s->acc, b, cudaMemcpyDeviceToHost, s->stream));
+  NB_CUDA(cudaStreamSynchronize(s->io_stream));
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s->ws, s->stream);
+}
 
 int nb_compute_forces(nb_sim* s, float* acc4) {
   if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");

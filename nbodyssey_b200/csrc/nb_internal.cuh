@@ -141,6 +141,7 @@ struct StepArgs {
   // writes part[t - t0] = a of sorted target t (no kick) instead of `acc`
   int t0, t1;
   float4* part;
+  cudaEvent_t after_prep;   // recorded after the prep kernel, or nullptr
 };
 
 // prep: [kick + drift] [+ bbox] [+ pack all-pairs sources] [+ zero sort scratch]

@@ -179,3 +179,25 @@ def test_invalid_params_on_live_sim():
         assert ei.value.code == L.NB_ERR_INVALID
         sim.step(1)
         sim.sync()
+
+
+@pytest.mark.parametrize("force", ["bh", "naive"])
+def test_step_host_equals_upload_step_download(force):
+    """nb_step_host (positions back on a second stream during the build and
+    walk) gives the same state as nb_set_state_acc + nb_step + downloads."""
+    pos, vel = ic.two_disks(30_000 if force == "bh" else 4_000, seed=51)
+    prm = api.SimParams(dt=0.005, epsilon=0.05, theta=0.5, force=force,
+                        traverse="warp")
+    with api.Simulation(pos, vel, prm) as sim:
+        acc = sim.compute_forces()
+        p, v, a = pos, vel, acc
+        for _ in range(3):
+            p, v, a = sim.step_host(p, v, a)
+    with api.Simulation(pos, vel, prm) as ref:
+        ra = ref.compute_forces()
+        rp, rv = pos, vel
+        for _ in range(3):
+            ref.set_state_acc(rp, rv, ra)
+            ref.step(1)
+            rp, rv, ra = ref.positions(), ref.velocities(), ref.accelerations()
+    assert np.array_equal(p, rp) and np.array_equal(v, rv) and np.array_equal(a, ra)
