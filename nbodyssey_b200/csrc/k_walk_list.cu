@@ -83,6 +83,9 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
   const float lox = warp_min(bi.x), loy = warp_min(bi.y), loz = warp_min(bi.z);
   const float hix = warp_max(bi.x), hiy = warp_max(bi.y), hiz = warp_max(bi.z);
   const float theta2 = a.theta2;
+  // the box test's thresholds with a 1e-5 relative margin, far above the
+  // few-ulp rounding of either side of the exact per-target test
+  const float th_lo = theta2 * 0.99999f, th_hi = theta2 * 1.00001f;
   if (!MASKED) {
     // the targets at the group's extremes (warp semantics: one rejecting
     // target opens a node for all)
@@ -189,17 +192,23 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
       cr = nd.right;
       s2 = nd.size2;
       const float cx = e.x, cy = e.y, cz = e.z;
-      const float ex = fmaxf(fmaxf(lox - cx, cx - hix), 0.f);
-      const float ey = fmaxf(fmaxf(loy - cy, cy - hiy), 0.f);
-      const float ez = fmaxf(fmaxf(loz - cz, cz - hiz), 0.f);
+      // per axis: distance below the box's low face and above its high face
+      // (at most one is positive); the nearest box point lies max(.., 0)
+      // away, the farthest max(|..|) away
+      const float lx = lox - cx, hx = cx - hix;
+      const float ly = loy - cy, hy = cy - hiy;
+      const float lz = loz - cz, hz = cz - hiz;
+      const float ex = fmaxf(fmaxf(lx, hx), 0.f);
+      const float ey = fmaxf(fmaxf(ly, hy), 0.f);
+      const float ez = fmaxf(fmaxf(lz, hz), 0.f);
       const float dmin2 = ex * ex + ey * ey + ez * ez;
-      const float fx = fmaxf(fabsf(cx - lox), fabsf(cx - hix));
-      const float fy = fmaxf(fabsf(cy - loy), fabsf(cy - hiy));
-      const float fz = fmaxf(fabsf(cz - loz), fabsf(cz - hiz));
+      const float fx = fmaxf(fabsf(lx), fabsf(hx));
+      const float fy = fmaxf(fabsf(ly), fabsf(hy));
+      const float fz = fmaxf(fabsf(lz), fabsf(hz));
       const float dmax2 = fx * fx + fy * fy + fz * fz;
-      if (s2 < theta2 * dmin2 * 0.99999f) {
+      if (s2 < th_lo * dmin2) {
         accm = M;
-      } else if (s2 > theta2 * dmax2 * 1.00001f) {
+      } else if (s2 > th_hi * dmax2) {
         accm = 0u;
       } else if (MASKED) {
         amb = true;
@@ -243,8 +252,10 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
         float t0, t1, z0, z1;
         up2(mul2(th2, d2), t0, t1);
         up2(B.y, z0, z1);
-        const unsigned b0 = __ballot_sync(full, !live || z0 < t0);
-        const unsigned b1 = __ballot_sync(full, !live || z1 < t1);
+        // a dead lane tests a copy of live target n-1 (warp semantics), and
+        // the candidate masks hold live lanes only (thread semantics)
+        const unsigned b0 = __ballot_sync(full, z0 < t0);
+        const unsigned b1 = __ballot_sync(full, z1 < t1);
         if (lane == 0) {
           sm.res[w][2 * q] = b0;
           sm.res[w][2 * q + 1] = b1;
