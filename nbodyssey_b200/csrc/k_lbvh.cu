@@ -141,7 +141,7 @@ __device__ __forceinline__ uint32_t digit_peers(uint32_t d, bool ok) {
 }
 
 template <typename K, int MODE>
-__global__ void __launch_bounds__(kSortThreads, 2)
+__global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
     k_sort_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                 K* __restrict__ kout, uint32_t* __restrict__ vout, int n,
                 int shift, const uint32_t* __restrict__ hist,

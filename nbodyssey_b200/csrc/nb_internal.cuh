@@ -52,8 +52,11 @@ constexpr int kStack = 128;
 
 // Onesweep sort geometry.
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+// 8 keys per thread and 4 CTAs per SM: at 1M keys a pass is one wave of
+// short tiles (a tile's latency, not bandwidth, sets the pass time)
+constexpr int kSortItems = 8;
+constexpr int kSortCtasPerSm = 4;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
 constexpr int kSortRadix = 256;
 
 // All-pairs source layout: particles are packed in pairs as two float4,
