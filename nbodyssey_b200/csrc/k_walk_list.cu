@@ -38,7 +38,8 @@ namespace nb {
 
 constexpr int kLW = 4;          // warps per block
 constexpr int kCand = 1024;     // candidate stack entries per warp
-constexpr int kList = 64;       // interaction-list entries per warp
+constexpr int kFlush = 32;      // list entries evaluated per flush
+constexpr int kList = 2 * kFlush;   // interaction-list entries per warp
 
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
@@ -107,7 +108,37 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
   int cnt = 0;
   float* ent = sm.ent[w];
 
-  // evaluates list entries [0, lc) for this lane's target
+  // list pair q (entries 2q, 2q+1) for this lane's target
+  auto pair_term = [&](int q) {
+    const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&ent[q * 8]);
+    const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&ent[q * 8 + 4]);
+    f2 m = B.y;
+    if (MASKED) {
+      const unsigned b0 = (sm.emask[w][2 * q] >> lane) & 1u;
+      const unsigned b1 = (sm.emask[w][2 * q + 1] >> lane) & 1u;
+      float m0, m1;
+      up2(B.y, m0, m1);
+      m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
+      if (COUNT) cnt += (int)(b0 + b1);
+    }
+    f2 dx = add2(A.x, nx);
+    f2 dy = add2(A.y, ny);
+    f2 dz = add2(B.x, nz);
+    f2 r2 = fma2(dz, dz, e2);
+    r2 = fma2(dy, dy, r2);
+    r2 = fma2(dx, dx, r2);
+    float r0, r1;
+    up2(r2, r0, r1);
+    f2 inv = pk2(mufu_rsqrt(r0), mufu_rsqrt(r1));
+    f2 wm = mul2(inv, m);
+    f2 i2 = mul2(inv, inv);
+    f2 f = mul2(wm, i2);
+    ax = fma2(dx, f, ax);
+    ay = fma2(dy, f, ay);
+    az = fma2(dz, f, az);
+  };
+  // evaluates list entries [0, lc) for this lane's target (the last, partial
+  // list of the walk)
   auto flush = [&](int lc) {
     if (lc & 1) {   // pad to a whole pair with a zero-mass entry
       if (lane == 0) {
@@ -118,36 +149,26 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
       __syncwarp();
     }
     const int np = (lc + 1) >> 1;
-    for (int q = 0; q < np; ++q) {
-      const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&ent[q * 8]);
-      const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&ent[q * 8 + 4]);
-      f2 m = B.y;
-      if (MASKED) {
-        const unsigned b0 = (sm.emask[w][2 * q] >> lane) & 1u;
-        const unsigned b1 = (sm.emask[w][2 * q + 1] >> lane) & 1u;
-        float m0, m1;
-        up2(B.y, m0, m1);
-        m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
-        if (COUNT) cnt += (int)(b0 + b1);
-      }
-      f2 dx = add2(A.x, nx);
-      f2 dy = add2(A.y, ny);
-      f2 dz = add2(B.x, nz);
-      f2 r2 = fma2(dz, dz, e2);
-      r2 = fma2(dy, dy, r2);
-      r2 = fma2(dx, dx, r2);
-      float r0, r1;
-      up2(r2, r0, r1);
-      f2 inv = pk2(mufu_rsqrt(r0), mufu_rsqrt(r1));
-      f2 wm = mul2(inv, m);
-      f2 i2 = mul2(inv, inv);
-      f2 f = mul2(wm, i2);
-      ax = fma2(dx, f, ax);
-      ay = fma2(dy, f, ay);
-      az = fma2(dz, f, az);
-    }
+    for (int q = 0; q < np; ++q) pair_term(q);
     if (!MASKED && COUNT) cnt += lc;
     __syncwarp();
+  };
+  // evaluates entries [0, kFlush) (unrolled: no loop counter, fixed
+  // offsets), then moves entries [kFlush, lc) to the front (lc < kFlush + 32);
+  // returns the new count
+  auto flush_full = [&](int lc) {
+#pragma unroll
+    for (int q = 0; q < kFlush / 2; ++q) pair_term(q);
+    if (!MASKED && COUNT) cnt += kFlush;
+    __syncwarp();
+    const int rest = lc - kFlush;   // 0 .. 31
+    if (lane < ((rest + 1) >> 1) * 2) {   // whole pairs, two float4 each
+      float4* v = reinterpret_cast<float4*>(ent);
+      v[lane] = v[kFlush + lane];
+    }
+    if (MASKED && lane < rest) sm.emask[w][lane] = sm.emask[w][kFlush + lane];
+    __syncwarp();
+    return rest;
   };
 
   int sp = 1, lc = 0;
@@ -301,10 +322,7 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
     }
     sp += 2 * __popc(pb);
     __syncwarp();
-    if (lc >= 32) {
-      flush(lc);
-      lc = 0;
-    }
+    if (lc >= kFlush) lc = flush_full(lc);
   }
 
   float3 ai;
