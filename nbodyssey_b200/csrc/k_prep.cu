@@ -169,7 +169,9 @@ int launch_prep(Workspace& w, const StepArgs& s, bool bbox, bool pack,
   a.zero_words = 0;
   if (bbox) {
     a.zero = w.hist;   // hist, tile counters and status are one allocation
-    a.zero_words = 8 * kSortRadix + 8 + 8 * w.status_tiles * kSortRadix;
+    // histograms, tile counters, and the tile status words of the passes
+    // this key width sorts with (pass p's words follow pass p - 1's)
+    a.zero_words = 8 * kSortRadix + 8 + sort_passes(s.key_bits) * w.status_tiles * kSortRadix;
   }
   int blocks = (npairs + kPrepThreads - 1) / kPrepThreads;
   if (blocks > kPrepMaxBlocks) blocks = kPrepMaxBlocks;
