@@ -56,21 +56,33 @@ __global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ pos,
   const bool wide = sizeof(K) == 8;
   const float scale = wide ? 2097152.f : 1024.f;
   const float qmax = scale - 1.f;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += gridDim.x * blockDim.x) {
-    float4 p = pos[i];
-    uint32_t qx = quantise(p.x, lx, inv, scale, qmax);
-    uint32_t qy = quantise(p.y, ly, inv, scale, qmax);
-    uint32_t qz = quantise(p.z, lz, inv, scale, qmax);
-    K k;
-    if (wide)
-      k = (K)((spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz));
-    else
-      k = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
-    keys[i] = k;
-    vals[i] = (uint32_t)i;
-    for (int ps = 0; ps < passes; ++ps)
-      atomicAdd(&s_hist[ps * kSortRadix + (uint32_t)((k >> (8 * ps)) & 0xffu)], 1u);
+  // four particles per thread and round, their loads issued together
+  const int stride = gridDim.x * blockDim.x;
+  for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    float4 pv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * stride;
+      if (i < n) pv[u] = pos[i];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + u * stride;
+      if (i >= n) break;
+      const float4 p = pv[u];
+      uint32_t qx = quantise(p.x, lx, inv, scale, qmax);
+      uint32_t qy = quantise(p.y, ly, inv, scale, qmax);
+      uint32_t qz = quantise(p.z, lz, inv, scale, qmax);
+      K k;
+      if (wide)
+        k = (K)((spread21(qx) << 2) | (spread21(qy) << 1) | spread21(qz));
+      else
+        k = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
+      keys[i] = k;
+      vals[i] = (uint32_t)i;
+      for (int ps = 0; ps < passes; ++ps)
+        atomicAdd(&s_hist[ps * kSortRadix + (uint32_t)((k >> (8 * ps)) & 0xffu)], 1u);
+    }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) {
