@@ -161,6 +161,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
                 const float4* __restrict__ pos, float4* __restrict__ pos_sorted,
                 const SimDesc* __restrict__ sims, int nsims) {
   constexpr int W = kSortThreads / 32;
+  static_assert(kSortThreads >= kSortRadix, "one thread per digit at least");
   __shared__ uint32_t s_wc[W][kSortRadix];
   __shared__ uint32_t s_base[kSortRadix];
   __shared__ uint32_t s_tex[kSortRadix];
@@ -175,8 +176,10 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
   if (tid == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
   for (int i = tid; i < W * kSortRadix; i += kSortThreads) (&s_wc[0][0])[i] = 0u;
 
+  // threads [0, kSortRadix) own one digit each in the per-digit steps
+  const bool dig = tid < kSortRadix;
   // global exclusive prefix of this pass's digit counts (one digit/thread)
-  const uint32_t h = hist[tid];
+  const uint32_t h = dig ? hist[tid] : 0u;
   uint32_t incl = h;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -221,11 +224,13 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
 
   // per digit: offsets of each warp inside the tile, and the tile's count
   uint32_t run = 0;
+  if (dig) {
 #pragma unroll
-  for (int w = 0; w < W; ++w) {
-    uint32_t c = s_wc[w][tid];
-    s_wc[w][tid] = run;
-    run += c;
+    for (int w = 0; w < W; ++w) {
+      uint32_t c = s_wc[w][tid];
+      s_wc[w][tid] = run;
+      run += c;
+    }
   }
   const uint32_t count = run;
   // tile-local start of digit tid in digit order
@@ -238,7 +243,9 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
   if (lane == 31) s_tsc[warp] = tin;
   uint32_t* my = status + (size_t)tile * kSortRadix + tid;
   uint32_t excl = 0;
-  if (tile == 0) {
+  if (!dig) {
+    // no digit of its own
+  } else if (tile == 0) {
     st_relaxed(my, kFlagInc | count);
   } else {
     st_relaxed(my, kFlagAgg | count);
@@ -280,10 +287,12 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
   uint32_t tofs = 0;
   for (int i = 0; i < warp; ++i) tofs += s_tsc[i];
   const uint32_t texcl = tofs + tin - count;
-  s_tex[tid] = texcl;
-  // global index of tile-local digit-order index i of digit d: s_base[d] + i
-  // (unsigned wrap-around cancels)
-  s_base[tid] = gexcl + excl - texcl;
+  if (dig) {
+    s_tex[tid] = texcl;
+    // global index of tile-local digit-order index i of digit d: s_base[d] + i
+    // (unsigned wrap-around cancels)
+    s_base[tid] = gexcl + excl - texcl;
+  }
   __syncthreads();
 
 #pragma unroll

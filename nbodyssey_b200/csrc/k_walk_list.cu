@@ -65,9 +65,21 @@ struct ListSmem {
   float4 ext[kLW][MASKED ? 1 : 6];        // targets of min / max x, y, z
 };
 
+// (v, v) in one 64-bit register pair, made at each use: volatile, so that
+// the compiler does not hoist the pairs and keep them live through the whole
+// walk (56 registers instead of 62: 9 resident blocks per SM instead of 8)
+__device__ __forceinline__ f2 pk2v(float v) {
+  f2 r;
+  asm volatile("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(v));
+  return r;
+}
+
 // The walk of warp `wg` (targets 32wg .. 32wg+31 of the tree in `a`); all
-// 32 lanes of the warp call it.
-template <bool MASKED, bool COUNT>
+// 32 lanes of the warp call it.  HOIST keeps the packed copies of the target
+// in registers for the whole walk (fewer registers the other way in the
+// single-tree kernel, more in the ensemble kernel, whose parameters are not
+// kernel constants).
+template <bool MASKED, bool COUNT, bool HOIST = false>
 __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
                                                ListSmem<MASKED>& sm) {
   const unsigned full = 0xffffffffu;
@@ -102,8 +114,11 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
   }
   const float cmx = 0.5f * (lox + hix), cmy = 0.5f * (loy + hiy), cmz = 0.5f * (loz + hiz);
 
-  const f2 nx = pk2(-bi.x, -bi.x), ny = pk2(-bi.y, -bi.y), nz = pk2(-bi.z, -bi.z);
-  const f2 e2 = pk2(a.eps2, a.eps2);
+  const float mx = -bi.x, my = -bi.y, mz = -bi.z;   // this lane's target, negated
+  const f2 hx = pk2(mx, mx), hy = pk2(my, my), hz = pk2(mz, mz), he2 = pk2(a.eps2, a.eps2);
+  auto px = [&]() { return HOIST ? hx : pk2v(mx); };
+  auto py = [&]() { return HOIST ? hy : pk2v(my); };
+  auto pz = [&]() { return HOIST ? hz : pk2v(mz); };
   f2 ax = 0ull, ay = 0ull, az = 0ull;
   int cnt = 0;
   float* ent = sm.ent[w];
@@ -121,10 +136,10 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
       m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
       if (COUNT) cnt += (int)(b0 + b1);
     }
-    f2 dx = add2(A.x, nx);
-    f2 dy = add2(A.y, ny);
-    f2 dz = add2(B.x, nz);
-    f2 r2 = fma2(dz, dz, e2);
+    f2 dx = add2(A.x, px());
+    f2 dy = add2(A.y, py());
+    f2 dz = add2(B.x, pz());
+    f2 r2 = fma2(dz, dz, HOIST ? he2 : pk2v(a.eps2));
     r2 = fma2(dy, dy, r2);
     r2 = fma2(dx, dx, r2);
     float r0, r1;
@@ -268,7 +283,7 @@ __device__ __forceinline__ void walk_list_warp(const WalkArgs& a, int wg,
       for (int q = 0; q < (na + 1) >> 1; ++q) {
         const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&sm.amb[w][q * 8]);
         const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&sm.amb[w][q * 8 + 4]);
-        const f2 dx = add2(A.x, nx), dy = add2(A.y, ny), dz = add2(B.x, nz);
+        const f2 dx = add2(A.x, px()), dy = add2(A.y, py()), dz = add2(B.x, pz());
         const f2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
         float t0, t1, z0, z1;
         up2(mul2(th2, d2), t0, t1);
@@ -384,7 +399,7 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list_ens(EnsArgs e) {
   a.t0 = 0;
   a.t1 = d.n;
   a.part = nullptr;
-  walk_list_warp<MASKED, false>(a, blk - d.base / 32, sm);
+  walk_list_warp<MASKED, false, true>(a, blk - d.base / 32, sm);
 }
 
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {

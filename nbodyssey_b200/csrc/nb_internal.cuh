@@ -51,12 +51,15 @@ struct __align__(16) Node {
 constexpr int kStack = 128;
 
 // Onesweep sort geometry.
-constexpr int kSortThreads = 256;
-// 8 keys per thread and 4 CTAs per SM: at 1M keys a pass is one wave of
-// short tiles (a tile's latency, not bandwidth, sets the pass time)
+// 512 threads (the first 256 own one digit each in the per-digit steps),
+// 8 keys per thread, 2 CTAs per SM: at 1M keys a pass is one wave of 245
+// tiles.  A tile's latency and the look-back's prefix propagation through
+// the tiles, not bandwidth, set the pass time; this geometry measured best
+// against 256 threads with 4096 or 2048 keys and 1024 keys per tile.
+constexpr int kSortThreads = 512;
 constexpr int kSortItems = 8;
-constexpr int kSortCtasPerSm = 4;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per tile
+constexpr int kSortCtasPerSm = 2;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr int kSortRadix = 256;
 
 // All-pairs source layout: particles are packed in pairs as two float4,

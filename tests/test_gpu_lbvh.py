@@ -53,8 +53,8 @@ def test_reference_fixture_bit_exact(golden_dir, bits):
     _assert_tree_equal(t, O.Tree(p4, bits), bits)
 
 
-# 1023 .. 3073 straddle the 1024-leaf groups of the bottom-up build, 2047 ..
-# 2049 and 4095 .. 4097 the sort's 2048-key tiles
+# 1023 .. 3073 straddle the 1024-leaf groups of the bottom-up build, 4095 ..
+# 4097 the sort's 4096-key tiles (2047 .. 2049 half a tile)
 @pytest.mark.parametrize("n", [2, 3, 31, 33, 1000, 1023, 1024, 1025, 2047, 2048, 2049,
                                3073, 4095, 4096, 4097, 100_003])
 @pytest.mark.parametrize("bits", [30, 63])
