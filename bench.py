@@ -9,10 +9,13 @@ centres of mass, warp walk with the closing kick fused.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-One JSON line on rank 0.  `value` = steps/s over the K timed steps (sum of
-per-step CUDA-event windows on the simulation's stream, L2 flushed by a
-256 MB write before every step, max over ranks; N ranks run N independent
-replicas).  `e2e` = the same metric through the C ABI with the state
+One JSON line on rank 0.  `value` = steps/s over the K timed steps, each
+step run as the library runs it by default (one captured CUDA graph per
+step); sum of per-step CUDA-event windows around the graph on the
+simulation's stream, L2 flushed by a 256 MB write before every step, max over
+ranks; N ranks run N independent replicas.  `phases_ms_per_step` comes from a
+second run of K steps launched kernel by kernel with events between the
+phases (`eager_steps_per_s`).  `e2e` = the same metric through the C ABI with the state
 (pos, vel, a(x)) uploaded from pinned host memory before and downloaded after
 every step.  `roofline` = the warp walk, useful work 20 flop x per-thread-
 criterion interactions, against the FP32 FMA peak measured on this GPU by a
@@ -331,29 +334,61 @@ def run_b200(args, rank, world, local, pg):
 
     inter0 = interactions(sim, api, params)
 
-    # warm-up (graph path), then timed steps with per-phase events
+    # warm-up: the step as the library runs it by default, one captured
+    # CUDA graph per step
     sim.step(args.warmup)
     sim.sync()
-    sim.reset_timing()
-    sim.set_timing(True)
     clocks = Clocks(local)
+    # the disks move, and the walk's cost with them: every measurement below
+    # starts from this state (pos, vel, a(x); the low position parts restart
+    # at zero)
+    snap = (sim.positions(), sim.velocities(), sim.accelerations())
+
+    def restore():
+        sim.set_state_acc(*snap)
+        sim.sync()
+
+    # timed steps (the headline): L2 flushed before every step, each step's
+    # graph bracketed by two CUDA events on the simulation's stream
     dist_barrier(pg)
     clocks.start()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        L.check(lib.nb_flush_l2(sim._h, L2_FLUSH_BYTES))
+        sim.record(2)
+        sim.step(1)
+        sim.record(3)
+        total_ms += sim.elapsed_ms(2, 3)
+    clk = clocks.stop()
+    dist_barrier(pg)
+    total_ms = dist_max(pg, total_ms)
+
+    # the same steps launched kernel by kernel with an event between phases,
+    # for the per-phase split (informational: the launches and events add
+    # time between the kernels)
+    restore()
+    sim.reset_timing()
+    sim.set_timing(True)
+    clocks.start(append=True)
     for _ in range(args.steps):
         L.check(lib.nb_flush_l2(sim._h, L2_FLUSH_BYTES))
         sim.step(1)
     sim.sync()
-    clk = clocks.stop()
+    clk = clocks.stop() or clk
     phases, calls = sim.phase_times()
-    total_ms, fcalls = sim.force_timing()
+    eager_ms, fcalls = sim.force_timing()
     sim.set_timing(False)
     assert calls == args.steps and fcalls == args.steps, (calls, fcalls)
     dist_barrier(pg)
-    total_ms = dist_max(pg, total_ms)
+    eager_ms = dist_max(pg, eager_ms)
     inter1 = interactions(sim, api, params)
     inter = 0.5 * (inter0 + inter1)
 
     # steady state through the captured graph, no flush (informational)
+    restore()
+    sim.step(1)
+    sim.sync()
+    restore()
     clocks.start(append=True)
     sim.record(0)
     sim.step(args.steps)
@@ -362,7 +397,9 @@ def run_b200(args, rank, world, local, pg):
     clk = clocks.stop() or clk
 
     # end to end: pinned host state in, one step, state out, every step
-    # (nb_step_host; each step's inputs are the previous step's outputs)
+    # (nb_step_host; each step's inputs are the previous step's outputs),
+    # from the same starting state
+    restore()
     keep = []
     bufs = [[pinned_array(lib, (n, 4), keep) for _ in range(3)] for _ in range(2)]
     L.check(lib.nb_get_positions(sim._h, L.ptr(bufs[0][0])))
@@ -403,7 +440,9 @@ def run_b200(args, rank, world, local, pg):
         "config": workload(args),
         "particle_steps_per_s": value * n,
         "graph_steps_per_s_no_flush": world * args.steps / (graph_ms * 1e-3),
+        "eager_steps_per_s": steps_total / (eager_ms * 1e-3),
         "phases_ms_per_step": {k: v / calls for k, v in phases.items() if v > 0},
+        "phases_path": "kernel-by-kernel launches with an event between phases",
         "interactions_per_particle": inter / n,
         # the step's kernels plus the L2-flush kernel before each step
         "gpu_launches": ((bh_kernels_per_step(n) if args.force == "bh" else 2) + 1)
