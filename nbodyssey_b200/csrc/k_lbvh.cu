@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
 
   // threads [0, kSortRadix) own one digit each in the per-digit steps
   const bool dig = tid < kSortRadix;
-  // global exclusive prefix of this pass's digit counts (one digit/thread)
+  // global exclusive prefix of this pass's digit counts (digit threads)
   const uint32_t h = dig ? hist[tid] : 0u;
   uint32_t incl = h;
 #pragma unroll
