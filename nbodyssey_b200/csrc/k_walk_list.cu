@@ -26,8 +26,9 @@
 //
 // Accepted nodes and leaves go to a shared-memory interaction list (pairs of
 // entries interleaved as (x0,x1,y0,y1)(z0,z1,m0,m1)) that the lanes evaluate
-// for their own target with packed FP32 math, two entries per instruction.
-// Entries whose mask excludes a lane contribute with mass 0.
+// for their own target with packed FP32 math, two entries per instruction,
+// in blocks of 32 entries by an unrolled body (the last, partial block by a
+// loop).  Entries whose mask excludes a lane contribute with mass 0.
 //
 // If the candidate stack would overflow, the warp falls back to the
 // depth-first walk of the same semantics (same interaction set).
