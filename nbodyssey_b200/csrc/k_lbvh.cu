@@ -40,8 +40,10 @@ __device__ __forceinline__ uint32_t quantise(float p, float lo, float inv,
   return (uint32_t)fminf(__fmul_rn(fmaxf(t, 0.f), scale), qmax);
 }
 
+constexpr int kMortonThreads = 1024;
+
 template <typename K>
-__global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ pos,
+__global__ void __launch_bounds__(kMortonThreads) k_morton(const float4* __restrict__ pos,
                                                 int n, const int* __restrict__ bbox,
                                                 K* keys, uint32_t* vals,
                                                 uint32_t* hist, int passes) {
@@ -93,14 +95,14 @@ __global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ pos,
 
 int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
   int passes = sort_passes(a.key_bits);
-  int blocks = (a.n + 255) / 256;
-  if (blocks > 2 * 148) blocks = 2 * 148;
+  int blocks = (a.n + kMortonThreads - 1) / kMortonThreads;
+  if (blocks > 148) blocks = 148;   // one CTA per SM: fewer histogram flushes
   if (a.key_bits == 63)
-    k_morton<uint64_t><<<blocks, 256, 0, st>>>(a.pos, a.n, w.bbox,
+    k_morton<uint64_t><<<blocks, kMortonThreads, 0, st>>>(a.pos, a.n, w.bbox,
                                                (uint64_t*)w.keys, w.vals, w.hist,
                                                passes);
   else
-    k_morton<uint32_t><<<blocks, 256, 0, st>>>(a.pos, a.n, w.bbox,
+    k_morton<uint32_t><<<blocks, kMortonThreads, 0, st>>>(a.pos, a.n, w.bbox,
                                                (uint32_t*)w.keys, w.vals, w.hist,
                                                passes);
   NB_CUDA(cudaGetLastError());
