@@ -218,10 +218,19 @@ NB_API int nb_leapfrog_step_dev(nb_workspace* w, int n, float* d_pos4, float* d_
  * each device looks up the array's device address; make that first call
  * before any stream capture.  Calls share the array: calls whose GPU work
  * overlaps race and must be serialised by the caller.  Asynchronous on
- * `stream`. */
+ * `stream`: device-side failures are not in its return code.  If a block of
+ * the kernel gives up waiting for its source tiles (NB_DEVERR_WAIT), its
+ * acceleration rows are written as NaN, never left stale. */
 NB_API int nb_compute_forces_naive_static(int n, const float* d_pos4,
                                           float* d_acc4, float eps, float G,
                                           void* stream);
+/* No counterpart in the reference.  Device status of the last
+ * nb_compute_forces_naive_static call on this device: waits for `stream`,
+ * copies the call's error word (NB_DEVERR_* bits) into *device_error (may be
+ * NULL) and returns NB_ERR_DEVICE when it is non-zero.  Allocates nothing;
+ * the next nb_compute_forces_naive_static call clears the word. */
+NB_API int nb_compute_forces_naive_static_status(unsigned* device_error,
+                                                 void* stream);
 /* No counterpart in the reference (one process drives one GPU there).  One
  * rank's share of compute_forces (src/forces.cuh:8) for a simulation split
  * over several GPUs: every rank holds the whole state and builds the whole

@@ -110,6 +110,7 @@ SIGNATURES = {
     "nb_leapfrog_step_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),
     "nb_total_energy_dev": (_I, [_P, _I, _P, _P, ctypes.POINTER(nb_params), _P, _P]),
     "nb_compute_forces_naive_static": (_I, [_I, _P, _P, _F, _F, _P]),
+    "nb_compute_forces_naive_static_status": (_I, [ctypes.POINTER(ctypes.c_uint), _P]),
     "nb_forces_range_dev": (_I, [_P, _I, _P, _P, _P, _P, _P, ctypes.POINTER(nb_params),
                                  _I, _I, _P]),
     "nb_forces_gather_dev": (_I, [_P, _I, _P, _P, _P, ctypes.POINTER(nb_params), _P]),

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -19,6 +20,26 @@ int set_error(int code, const std::string& msg) {
   return code;
 }
 const char* last_error() { return g_err.c_str(); }
+
+int device_sm_count() {
+  static std::mutex mu;
+  static int count[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    cudaGetLastError();
+    return 148;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!count[dev]) {
+    int c = 0;
+    if (cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0) {
+      cudaGetLastError();
+      c = 148;
+    }
+    count[dev] = c;
+  }
+  return count[dev];
+}
 
 // ---------------------------------------------------------------------------
 // Workspace

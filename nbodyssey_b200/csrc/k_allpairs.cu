@@ -106,13 +106,14 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
   }
   const f2 e2 = pk2(a.eps2, a.eps2);
 
-  bool ok = true;
+  // A thread whose barrier wait gives up still runs the tile (shared-memory
+  // reads of a tile that has not landed are harmless; the results are
+  // discarded), so the barrier at the end of the tile is reached by every
+  // thread and the decision to leave is the whole block's.
+  int failed_at = -1;
   for (int t = 0; t < ntiles; ++t) {
     const int s = t % kStages;
-    if (!mbar_wait(&s_bar[s], (uint32_t)((t / kStages) & 1))) {
-      ok = false;
-      break;
-    }
+    const bool landed = mbar_wait(&s_bar[s], (uint32_t)((t / kStages) & 1));
     const ulonglong2* tile = reinterpret_cast<const ulonglong2*>(s_tile[s]);
 #pragma unroll 4
     for (int q = 0; q < kSrcTile / 2; ++q) {
@@ -137,23 +138,35 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
         az[k] = fma2(dz, f, az[k]);
       }
     }
-    __syncthreads();   // every thread is done with stage s
+    // every thread is done with stage s; leave together if any wait gave up
+    if (__syncthreads_or(!landed)) {
+      failed_at = t;
+      break;
+    }
     if (tid == 0 && t + kStages < ntiles)
       bulk_load(s_tile[s], a.src + 2 * ((j0 + (t + kStages) * kSrcTile) / 2),
                 kTileBytes, &s_bar[s]);
   }
-  if (!ok) {
-    if (tid == 0) raise_err(a.err, NB_DEVERR_WAIT);
-    return;
+  const bool ok = failed_at < 0;
+  if (!ok && tid == 0) {
+    raise_err(a.err, NB_DEVERR_WAIT);
+    // let the copies still in flight into this block's shared memory land
+    // (bounded waits) before the block retires
+    for (int t = failed_at; t < ntiles && t < failed_at + kStages; ++t)
+      mbar_wait(&s_bar[t % kStages], (uint32_t)((t / kStages) & 1));
   }
 
+  // A block that could not read its sources writes NaN rows (and, with the
+  // j-split, still takes its ticket), so a failed launch leaves visibly
+  // invalid accelerations and a consistent ticket counter, never stale rows.
+  const float bad = __int_as_float(0x7fc00000);
   float3 res[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     float u, v;
-    up2(ax[k], u, v); res[k].x = u + v;
-    up2(ay[k], u, v); res[k].y = u + v;
-    up2(az[k], u, v); res[k].z = u + v;
+    up2(ax[k], u, v); res[k].x = ok ? u + v : bad;
+    up2(ay[k], u, v); res[k].y = ok ? u + v : bad;
+    up2(az[k], u, v); res[k].z = ok ? u + v : bad;
   }
 
   if (a.jsplit > 1) {
@@ -204,7 +217,7 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
 }
 
 // Geometry: 256 threads x 4 targets per CTA; the source range is split so the
-// grid fills the 148 SMs (two CTAs each) several times over.
+// grid fills the SMs (two CTAs each) several times over.
 APGeom allpairs_geometry(int n) {
   APGeom g;
   g.threads = 256;
@@ -213,7 +226,7 @@ APGeom allpairs_geometry(int n) {
   g.itiles = (n + per - 1) / per;
   const int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
   const int jtiles = npad / kSrcTile;
-  const int target = 148 * 2 * 4;   // CTAs wanted in flight over the launch
+  const int target = device_sm_count() * 2 * 4;   // CTAs wanted in flight over the launch
   int js = (target + g.itiles - 1) / g.itiles;
   if (js > jtiles) js = jtiles;
   if (js < 1) js = 1;
@@ -344,14 +357,15 @@ __global__ void __launch_bounds__(kEThreads) k_energy_reduce(
 int launch_energy(Workspace& w, int n, const float4* pos, const float4* vel,
                   float eps2, float G, cudaStream_t st) {
   const int itiles = (n + kEThreads - 1) / kEThreads;
-  int js = (148 * 4 + itiles - 1) / itiles;
+  const int sms = device_sm_count();
+  int js = (sms * 4 + itiles - 1) / itiles;
   const int jt = (n + kETile - 1) / kETile;
   if (js > jt) js = jt;
   if (js < 1) js = 1;
   int jchunk = (jt + js - 1) / js * kETile;
   js = (n + jchunk - 1) / jchunk;
   int rblocks = (n + kEThreads - 1) / kEThreads;
-  if (rblocks > 296) rblocks = 296;
+  if (rblocks > 2 * sms) rblocks = 2 * sms;
   NB_TRY(ws_reserve_energy(w, n, rblocks, js));
   k_energy_phi<<<dim3(itiles, js), kEThreads, 0, st>>>(pos, n, eps2, jchunk,
                                                         w.ephi);
@@ -388,6 +402,7 @@ constexpr int kStaticMaxSplit = 8;
 constexpr size_t kStaticSrcBytes = (size_t)kStaticMaxN * sizeof(float4);
 constexpr size_t kStaticPartBytes = (size_t)kStaticMaxSplit * kStaticMaxN * sizeof(float4);
 constexpr size_t kStaticTailBytes = 256;   // tickets (<= 33 words) + error word
+constexpr int kStaticErrWord = 48;          // word index of the error word in the tail
 static __device__ __align__(256) unsigned char
     g_static_scratch[kStaticSrcBytes + kStaticPartBytes + kStaticTailBytes];
 
@@ -475,8 +490,30 @@ extern "C" int nb_compute_forces_naive_static(int n, const float* d_pos4,
   a.vel = nullptr;
   a.part = part;
   a.tickets = tail;
-  a.err = tail + 48;
+  a.err = tail + kStaticErrWord;
   k_allpairs<256, 4><<<dim3(g.itiles, js), 256, 0, st>>>(a);
   NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+extern "C" int nb_compute_forces_naive_static_status(unsigned* device_error,
+                                                     void* stream) {
+  using namespace nb;
+  unsigned char* base = nullptr;
+  NB_TRY(static_scratch_address(&base));
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned* word =
+      (const unsigned*)(base + kStaticSrcBytes + kStaticPartBytes) + kStaticErrWord;
+  unsigned e = 0;
+  NB_CUDA(cudaMemcpyAsync(&e, word, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(st));
+  if (device_error) *device_error = e;
+  if (e)
+    return set_error(NB_ERR_DEVICE,
+                     "nb_compute_forces_naive_static: device error word 0x" +
+                         std::to_string(e) +
+                         (e & NB_DEVERR_WAIT ? " (bulk-copy barrier wait limit; the rows "
+                                               "of the blocks that gave up are NaN)"
+                                             : ""));
   return NB_OK;
 }

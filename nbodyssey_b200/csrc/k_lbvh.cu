@@ -96,7 +96,8 @@ __global__ void __launch_bounds__(kMortonThreads) k_morton(const float4* __restr
 int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
   int passes = sort_passes(a.key_bits);
   int blocks = (a.n + kMortonThreads - 1) / kMortonThreads;
-  if (blocks > 148) blocks = 148;   // one CTA per SM: fewer histogram flushes
+  const int sms = device_sm_count();
+  if (blocks > sms) blocks = sms;   // one CTA per SM: fewer histogram flushes
   if (a.key_bits == 63)
     k_morton<uint64_t><<<blocks, kMortonThreads, 0, st>>>(a.pos, a.n, w.bbox,
                                                (uint64_t*)w.keys, w.vals, w.hist,
@@ -1039,7 +1040,7 @@ __global__ void __launch_bounds__(256) k_ens_morton(EnsArgs e) {
 
 int launch_ens_morton(const EnsArgs& e, cudaStream_t st) {
   int blocks = (e.nslots + 255) / 256;
-  if (blocks > 4 * 148) blocks = 4 * 148;
+  if (blocks > 4 * device_sm_count()) blocks = 4 * device_sm_count();
   k_ens_morton<<<blocks, 256, 0, st>>>(e);
   NB_CUDA(cudaGetLastError());
   return NB_OK;

@@ -312,7 +312,7 @@ int launch_ens_prep(const EnsArgs& e, cudaStream_t st) {
   NB_CUDA(cudaMemsetAsync(e.bbox_max, 0x80, sizeof(int) * 4 * e.nsims, st));
   const int zero_words = 8 * kSortRadix + 8 + 8 * e.status_tiles * kSortRadix;
   int blocks = (e.nslots + kPrepThreads - 1) / kPrepThreads;
-  if (blocks > 4 * 148) blocks = 4 * 148;
+  if (blocks > 4 * device_sm_count()) blocks = 4 * device_sm_count();
   if (blocks < 1) blocks = 1;
   if (e.kick_drift)
     k_ens_prep<true><<<blocks, kPrepThreads, 0, st>>>(e, e.hist, zero_words);
@@ -331,7 +331,7 @@ __global__ void k_flush(uint4* buf, size_t n) {
 }
 
 int launch_flush(void* buf, size_t bytes, cudaStream_t st) {
-  k_flush<<<148 * 8, 256, 0, st>>>((uint4*)buf, bytes / sizeof(uint4));
+  k_flush<<<device_sm_count() * 8, 256, 0, st>>>((uint4*)buf, bytes / sizeof(uint4));
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }

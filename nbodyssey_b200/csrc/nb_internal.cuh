@@ -169,6 +169,9 @@ int launch_allpairs(Workspace& w, const StepArgs& a, cudaStream_t st);
 int launch_energy(Workspace& w, int n, const float4* pos, const float4* vel,
                   float eps2, float G, cudaStream_t st);
 int launch_flush(void* buf, size_t bytes, cudaStream_t st);
+// Streaming multiprocessors of the current device (read once per device;
+// 148 on a B200), for grid sizes that should fill the device.
+int device_sm_count();
 int measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
 
 // all-pairs launch geometry (autotuned by n)

@@ -2,7 +2,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Runs only where the nbodyssey sources are present (pass their path with
---reference, default /root/reference).  It imports the reference's Python
+--reference, required).  It imports the reference's Python
 oracles -- scripts/lbvh_check.py, scripts/reference_nbody.py,
 scripts/barnes_hut_reference.py, scripts/generate_ic.py -- calls their
 functions unmodified, runs reference_nbody.py as a program, and stores the
@@ -172,7 +172,8 @@ def octree_fixture(gen, bhr):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="checkout of the nbodyssey reference")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(args.reference, "scripts"))
     import barnes_hut_reference as bhr

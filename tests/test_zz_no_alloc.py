@@ -44,6 +44,10 @@ def test_static_scratch_forces_match_allocating_path():
             L.check(lib.nb_compute_forces_naive_static(
                 n, ctypes.c_void_p(dpos.data_ptr()),
                 ctypes.c_void_p(d_static.data_ptr()), EPS, 1.0, stream))
+            # the call's device status: no block gave up on its source tiles
+            word = ctypes.c_uint(0xFFFFFFFF)
+            L.check(lib.nb_compute_forces_naive_static_status(ctypes.byref(word), stream))
+            assert word.value == 0
             prm = api.SimParams(epsilon=EPS, force="naive").to_c()
             L.check(lib.nb_compute_forces_dev(
                 ws, n, ctypes.c_void_p(dpos.data_ptr()),
