@@ -80,7 +80,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--force", choices=["bh", "naive"], default="bh",
                     help="naive: time the all-pairs module instead (e.g. --n 262144)")
-    ap.add_argument("--walk", choices=["list", "dfs"], default="list",
+    ap.add_argument("--walk", choices=["pair", "list", "dfs"], default="pair",
                     help="tree-walk kernel: batched list walk or depth-first walk")
     ap.add_argument("--workload", choices=["single", "ensemble", "serve"],
                     default="single",
@@ -452,7 +452,8 @@ def run_b200(args, rank, world, local, pg):
                 "path": "nb_step_host: pinned host pos / vel / a(x) in, one step, "
                         "pos / vel / a(x_new) out (positions return on a second "
                         "stream during the tree build and walk), wall clock"},
-        "roofline": {"kernel": (("k_walk_list" if args.walk == "list" else "k_walk_%s" % args.traverse) if args.force == "bh"
+        "roofline": {"kernel": ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
+                                    args.walk, "k_walk_%s" % args.traverse) if args.force == "bh"
                                 else "k_allpairs"), "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic,

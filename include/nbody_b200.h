@@ -328,6 +328,31 @@ NB_API int nb_server_get_stats(nb_server* s, nb_server_stats* out);
 /* load_ic (src/main.cu:115-128).  Call with pos4 = vel4 = NULL to get n. */
 NB_API int nb_read_ic(const char* path, int* n, float* pos4, float* vel4);
 NB_API int nb_write_ic(const char* path, int n, const float* pos4, const float* vel4);
+/* State files (checkpoint / resume; the reference has none, its runs restart
+ * only from an ic.bin).  The file is the ic.bin layout of docs/FORMATS.md:8-16
+ * (int32 n, float4 pos[n], float4 vel[n]) -- any ic.bin reader, load_ic
+ * (src/main.cu:115-128) included, takes it as initial conditions -- followed
+ * by a trailer: the magic "NBSTATE1", int32 flags (NB_STATE_*), the run's
+ * nb_params, float4 pos_lo[n] (low-order position parts of the compensated
+ * drift) and float4 acc[n] (a(x) of the stored positions).  A run resumed
+ * from it continues bit for bit as if it had not stopped. */
+#define NB_STATE_TRAILER 1 /* the trailer is present (0: a plain ic.bin) */
+#define NB_STATE_ACC 2     /* acc[] holds a(x) of the stored positions */
+#define NB_STATE_LO 4      /* pos_lo[] holds low-order position parts */
+NB_API int nb_write_state_file(const char* path, int n, const float* pos4,
+                               const float* vel4, const float* lo4,
+                               const float* acc4, const nb_params* p);
+/* Call with pos4 = vel4 = NULL to get n.  A plain ic.bin gives flags = 0,
+ * zero lo4 / acc4 and leaves *p unchanged.  lo4, acc4, p, flags may be NULL. */
+NB_API int nb_read_state_file(const char* path, int* n, float* pos4, float* vel4,
+                              float* lo4, float* acc4, nb_params* p, int* flags);
+/* Writes the simulation's state (positions with their low-order parts,
+ * velocities, a(x) when it is current, parameters) as a state file. */
+NB_API int nb_save_state(nb_sim* s, const char* path);
+/* Replaces the simulation's state from a state file (n must match) and takes
+ * its parameters; with a(x) stored the next step needs no priming force
+ * evaluation.  A plain ic.bin loads like nb_set_state. */
+NB_API int nb_load_state(nb_sim* s, const char* path);
 /* dump_frame (src/main.cu:130-138): <dir>/frame_%05d.bin. */
 NB_API int nb_write_frame(const char* dir, int index, int n, const float* pos4);
 /* One energy-log row, "%d,%.5f,%.8e,%.8e,%.8e,%.3e\n" with time = step*dt

@@ -28,6 +28,9 @@ NB_AUTO_CROSSOVER = 20000
 NB_TRAVERSE_THREAD = 0
 NB_TRAVERSE_WARP = 1
 NB_PHASES = 8
+NB_STATE_TRAILER = 1
+NB_STATE_ACC = 2
+NB_STATE_LO = 4
 PHASE_NAMES = ("prep", "morton", "sort", "build", "com", "walk", "energy", "other")
 
 
@@ -137,6 +140,11 @@ SIGNATURES = {
     "nb_read_ic": (_I, [_S, ctypes.POINTER(_I), _P, _P]),
     "nb_write_ic": (_I, [_S, _I, _P, _P]),
     "nb_write_frame": (_I, [_S, _I, _I, _P]),
+    "nb_write_state_file": (_I, [_S, _I, _P, _P, _P, _P, ctypes.POINTER(nb_params)]),
+    "nb_read_state_file": (_I, [_S, ctypes.POINTER(_I), _P, _P, _P, _P,
+                                ctypes.POINTER(nb_params), ctypes.POINTER(_I)]),
+    "nb_save_state": (_I, [_P, _S]),
+    "nb_load_state": (_I, [_P, _S]),
     "nb_format_energy_row": (_I, [_P, _SZ, _I, _F, _D, _D, _D, _D]),
     "nb_run": (_I, [_P, _I, _I, _S, _S, _I, ctypes.POINTER(nb_run_stats)]),
 }

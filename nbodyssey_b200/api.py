@@ -44,7 +44,7 @@ class SimParams:
     traverse: str = BhTraversal.THREAD
     key_bits: int = 30
     compensated: bool = True
-    walk_kernel: str = "list"   # "list" (batched, default) or "dfs"
+    walk_kernel: str = "pair"   # "pair" (child-pair records, default), "dfs" or "list"
 
     def to_c(self):
         if self.force not in (ForceMethod.NAIVE, ForceMethod.BARNES_HUT, ForceMethod.AUTO):
@@ -61,10 +61,21 @@ class SimParams:
         p.traverse = L.NB_TRAVERSE_WARP if self.traverse == BhTraversal.WARP else L.NB_TRAVERSE_THREAD
         p.key_bits = int(self.key_bits)
         p.compensated = 1 if self.compensated else 0
-        if self.walk_kernel not in ("list", "dfs"):
-            raise ValueError("walk_kernel must be list or dfs")
-        p.walk_kernel = 0 if self.walk_kernel == "list" else 1
+        if self.walk_kernel not in ("pair", "dfs", "list"):
+            raise ValueError("walk_kernel must be pair, dfs or list")
+        p.walk_kernel = {"pair": 0, "dfs": 1, "list": 2}[self.walk_kernel]
         return p
+
+    @classmethod
+    def from_c(cls, p):
+        """The SimParams of a C nb_params."""
+        force = {L.NB_FORCE_NAIVE: ForceMethod.NAIVE, L.NB_FORCE_BH: ForceMethod.BARNES_HUT,
+                 L.NB_FORCE_AUTO: ForceMethod.AUTO}[p.force]
+        return cls(dt=p.dt, epsilon=p.eps, G=p.G, theta=p.theta, force=force,
+                   traverse=BhTraversal.WARP if p.traverse == L.NB_TRAVERSE_WARP
+                   else BhTraversal.THREAD,
+                   key_bits=p.key_bits, compensated=bool(p.compensated),
+                   walk_kernel={0: "pair", 1: "dfs", 2: "list"}[p.walk_kernel])
 
 
 def _rows4(a, name):
@@ -72,6 +83,36 @@ def _rows4(a, name):
     if a.ndim != 2 or a.shape[1] != 4:
         raise ValueError("%s must be an (n, 4) float32 array" % name)
     return a
+
+
+def read_state(path):
+    """A state file (checkpoint) or plain ic.bin: dict with pos, vel, lo, acc
+    ((n, 4) float32), params (SimParams, None for a plain ic.bin) and flags
+    (NB_STATE_* bits)."""
+    lib = L.load()
+    n = ctypes.c_int(0)
+    L.check(lib.nb_read_state_file(path.encode(), ctypes.byref(n), None, None, None,
+                                   None, None, None))
+    pos, vel, lo, acc = (np.empty((n.value, 4), np.float32) for _ in range(4))
+    prm = L.nb_params()
+    flags = ctypes.c_int(0)
+    L.check(lib.nb_read_state_file(path.encode(), ctypes.byref(n), L.ptr(pos), L.ptr(vel),
+                                   L.ptr(lo), L.ptr(acc), ctypes.byref(prm),
+                                   ctypes.byref(flags)))
+    params = SimParams.from_c(prm) if flags.value & L.NB_STATE_TRAILER else None
+    return {"pos": pos, "vel": vel, "lo": lo, "acc": acc, "params": params,
+            "flags": flags.value}
+
+
+def write_state(path, pos4, vel4, params: SimParams, lo4=None, acc4=None):
+    """Writes a state file from host arrays (lo4 / acc4 may be None)."""
+    pos4 = _rows4(pos4, "pos4")
+    vel4 = _rows4(vel4, "vel4")
+    lo4 = None if lo4 is None else _rows4(lo4, "lo4")
+    acc4 = None if acc4 is None else _rows4(acc4, "acc4")
+    L.check(L.load().nb_write_state_file(path.encode(), pos4.shape[0], L.ptr(pos4),
+                                         L.ptr(vel4), L.ptr(lo4), L.ptr(acc4),
+                                         ctypes.byref(params.to_c())))
 
 
 def device_count():
@@ -127,6 +168,28 @@ class Simulation:
         if pos4.shape[0] != self.n or vel4.shape[0] != self.n:
             raise ValueError("state must keep n = %d" % self.n)
         L.check(self._lib.nb_set_state(self._h, L.ptr(pos4), L.ptr(vel4)))
+
+    @classmethod
+    def from_state(cls, path):
+        """A simulation resumed from a state file written by save_state: the
+        stored parameters, positions with their low-order parts, velocities
+        and a(x); it continues bit for bit as the run that wrote it."""
+        st = read_state(path)
+        sim = cls(st["pos"], st["vel"], st["params"] or SimParams())
+        sim.load_state(path)
+        return sim
+
+    def save_state(self, path):
+        """Checkpoint: the state file (ic.bin layout + trailer) of this
+        simulation's current state."""
+        L.check(self._lib.nb_save_state(self._h, path.encode()))
+
+    def load_state(self, path):
+        """Replaces the state (and, from a state file, the parameters)."""
+        L.check(self._lib.nb_load_state(self._h, path.encode()))
+        p = L.nb_params()
+        L.check(self._lib.nb_get_params(self._h, ctypes.byref(p)))
+        self.params = SimParams.from_c(p)
 
     def _get(self, fn):
         out = np.empty((self.n, 4), np.float32)

@@ -94,6 +94,7 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_TRY(dalloc(&w.vals_alt, cap));
   NB_TRY(dalloc(&w.pos_sorted, cap));
   NB_TRY(dalloc(&w.nodes, ni));
+  NB_TRY(dalloc(&w.pairs, ni));
   NB_TRY(dalloc(&w.parent, 2 * (size_t)cap));
   for (int i = 0; i < 2; ++i) {
     NB_TRY(dalloc(&w.seg[i], build_seg_entries(cap)));
@@ -108,6 +109,7 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_CUDA(cudaMemset(w.vals_alt, 0, cap * sizeof(uint32_t)));
   NB_CUDA(cudaMemset(w.parent, 0xff, 2 * (size_t)cap * sizeof(int)));
   NB_CUDA(cudaMemset(w.nodes, 0, ni * sizeof(Node)));
+  NB_CUDA(cudaMemset(w.pairs, 0, ni * sizeof(PairRec)));
   w.status_tiles = (cap + kSortTile - 1) / kSortTile;
   size_t words = 8 * kSortRadix + 8 + (size_t)8 * w.status_tiles * kSortRadix;
   NB_TRY(dalloc(&w.hist, words));
@@ -156,7 +158,7 @@ int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit) {
 
 void ws_free(Workspace& w) {
   cudaFree(w.keys); cudaFree(w.keys_alt); cudaFree(w.vals); cudaFree(w.vals_alt);
-  cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.parent);
+  cudaFree(w.pos_sorted); cudaFree(w.nodes); cudaFree(w.pairs); cudaFree(w.parent);
   for (int i = 0; i < 2; ++i) { cudaFree(w.seg[i]); cudaFree(w.seg_count[i]); }
   cudaFree(w.sums); cudaFree(w.box_lo); cudaFree(w.box_hi); cudaFree(w.hist);
   cudaFree(w.bbox); cudaFree(w.bbox_part); cudaFree(w.bbox_ticket);
@@ -185,7 +187,7 @@ static int check_params(const nb_params* p) {
     return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
   if (p->key_bits != 30 && p->key_bits != 63)
     return set_error(NB_ERR_INVALID, "key_bits must be 30 or 63");
-  if (p->walk_kernel != 0 && p->walk_kernel != 1)
+  if (p->walk_kernel != 0 && p->walk_kernel != 1 && p->walk_kernel != 2)
     return set_error(NB_ERR_INVALID, "walk_kernel must be 0 or 1");
   return NB_OK;
 }
@@ -641,6 +643,41 @@ int nb_get_accelerations(nb_sim* s, float* acc4) { return download(s, acc4, s ? 
 int nb_get_positions(nb_sim* s, float* pos4) { return download(s, pos4, s ? s->pos : nullptr); }
 int nb_get_velocities(nb_sim* s, float* vel4) { return download(s, vel4, s ? s->vel : nullptr); }
 int nb_get_position_lo(nb_sim* s, float* lo4) { return download(s, lo4, s ? s->pos_lo : nullptr); }
+
+int nb_save_state(nb_sim* s, const char* path) {
+  if (!s || !path) return set_error(NB_ERR_INVALID, "NULL argument");
+  const size_t rows = (size_t)s->n * 4;
+  std::vector<float> pos(rows), vel(rows), lo(rows), acc(rows);
+  NB_TRY(nb_get_positions(s, pos.data()));
+  NB_TRY(nb_get_velocities(s, vel.data()));
+  NB_TRY(nb_get_position_lo(s, lo.data()));
+  if (s->primed) NB_TRY(nb_get_accelerations(s, acc.data()));
+  return nb_write_state_file(path, s->n, pos.data(), vel.data(), lo.data(),
+                             s->primed ? acc.data() : nullptr, &s->p);
+}
+
+int nb_load_state(nb_sim* s, const char* path) {
+  if (!s || !path) return set_error(NB_ERR_INVALID, "NULL argument");
+  int cnt = 0;
+  NB_TRY(nb_read_state_file(path, &cnt, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr));
+  if (cnt != s->n)
+    return set_error(NB_ERR_INVALID, "state file holds " + std::to_string(cnt) +
+                                         " particles, the simulation " + std::to_string(s->n));
+  const size_t rows = (size_t)s->n * 4;
+  std::vector<float> pos(rows), vel(rows), lo(rows), acc(rows);
+  nb_params p = s->p;
+  int flags = 0;
+  NB_TRY(nb_read_state_file(path, &cnt, pos.data(), vel.data(), lo.data(), acc.data(), &p,
+                            &flags));
+  if (flags & NB_STATE_TRAILER) NB_TRY(nb_set_params(s, &p));
+  if (flags & NB_STATE_ACC) NB_TRY(nb_set_state_acc(s, pos.data(), vel.data(), acc.data()));
+  else NB_TRY(nb_set_state(s, pos.data(), vel.data()));
+  if (flags & NB_STATE_LO)
+    NB_CUDA(cudaMemcpyAsync(s->pos_lo, lo.data(), sizeof(float4) * s->n,
+                            cudaMemcpyHostToDevice, s->stream));
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  return NB_OK;
+}
 
 int nb_step_host(nb_sim* s, const float* pos4, const float* vel4, const float* acc4,
                  float* pos_out4, float* vel_out4, float* acc_out4) {

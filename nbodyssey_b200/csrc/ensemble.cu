@@ -198,6 +198,7 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if ((rc = ens_alloc(h, &e.perm, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.perm_alt, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.nodes, S)) != NB_OK) break;
+    if ((rc = ens_alloc(h, &e.pairs, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.parent, 2 * S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.sums, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.box_lo, S)) != NB_OK) break;
@@ -235,6 +236,7 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.perm_alt, 0, S * 4, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.parent, 0xff, 2 * S * 4, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.nodes, 0, S * sizeof(Node), st);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(e.pairs, 0, S * sizeof(PairRec), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.hist, 0, words * 4, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.err, 0, 16, st);
     if (ce == cudaSuccess)

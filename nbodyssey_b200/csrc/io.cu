@@ -89,6 +89,71 @@ int nb_write_ic(const char* path, int n, const float* pos4, const float* vel4) {
   return NB_OK;
 }
 
+// State file: the ic.bin layout (int32 n, float4 pos[n], float4 vel[n],
+// docs/FORMATS.md:8-16), so any ic.bin reader takes it as initial
+// conditions, followed by a trailer that makes a resumed run continue bit for
+// bit: the 8-byte magic "NBSTATE1", int32 flags (NB_STATE_*), the run's
+// nb_params, float4 pos_lo[n] (low-order position parts) and float4 acc[n]
+// (a(x) of the stored positions).
+static const char kStateMagic[8] = {'N', 'B', 'S', 'T', 'A', 'T', 'E', '1'};
+
+int nb_write_state_file(const char* path, int n, const float* pos4, const float* vel4,
+                        const float* lo4, const float* acc4, const nb_params* p) {
+  if (!path || !pos4 || !vel4 || !p || n <= 0) return set_error(NB_ERR_INVALID, "bad argument");
+  NB_TRY(mkdirs(parent_dir(path)));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_error(NB_ERR_IO, std::string("cannot open ") + path);
+  int32_t cnt = n;
+  int32_t flags = NB_STATE_TRAILER | (acc4 ? NB_STATE_ACC : 0) | (lo4 ? NB_STATE_LO : 0);
+  std::vector<float> zero(acc4 && lo4 ? 0 : (size_t)n * 4, 0.f);
+  bool ok = std::fwrite(&cnt, 4, 1, f) == 1 &&
+            std::fwrite(pos4, 16, (size_t)n, f) == (size_t)n &&
+            std::fwrite(vel4, 16, (size_t)n, f) == (size_t)n &&
+            std::fwrite(kStateMagic, 1, 8, f) == 8 && std::fwrite(&flags, 4, 1, f) == 1 &&
+            std::fwrite(p, sizeof(nb_params), 1, f) == 1 &&
+            std::fwrite(lo4 ? lo4 : zero.data(), 16, (size_t)n, f) == (size_t)n &&
+            std::fwrite(acc4 ? acc4 : zero.data(), 16, (size_t)n, f) == (size_t)n;
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return set_error(NB_ERR_IO, std::string("write failed: ") + path);
+  return NB_OK;
+}
+
+int nb_read_state_file(const char* path, int* n, float* pos4, float* vel4, float* lo4,
+                       float* acc4, nb_params* p, int* flags) {
+  if (!path || !n) return set_error(NB_ERR_INVALID, "NULL argument");
+  if (!pos4 && !vel4) return nb_read_ic(path, n, nullptr, nullptr);
+  int cnt = *n;
+  NB_TRY(nb_read_ic(path, &cnt, pos4, vel4));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_error(NB_ERR_IO, std::string("cannot open ") + path);
+  const long off = 4 + 32L * cnt;
+  char magic[8] = {};
+  int32_t fl = 0;
+  nb_params q{};
+  bool trailer = std::fseek(f, off, SEEK_SET) == 0 && std::fread(magic, 1, 8, f) == 8 &&
+                 std::memcmp(magic, kStateMagic, 8) == 0;
+  bool ok = true;
+  if (trailer) {
+    const size_t want = (size_t)cnt * 4;
+    std::vector<float> tmp(want);
+    ok = std::fread(&fl, 4, 1, f) == 1 && std::fread(&q, sizeof(nb_params), 1, f) == 1 &&
+         std::fread(lo4 ? lo4 : tmp.data(), sizeof(float), want, f) == want &&
+         std::fread(acc4 ? acc4 : tmp.data(), sizeof(float), want, f) == want;
+  }
+  std::fclose(f);
+  if (!ok) return set_error(NB_ERR_IO, std::string("truncated state trailer: ") + path);
+  if (!trailer) {   // a plain ic.bin: no low-order parts, no a(x)
+    fl = 0;
+    if (lo4) std::memset(lo4, 0, sizeof(float) * 4 * (size_t)cnt);
+    if (acc4) std::memset(acc4, 0, sizeof(float) * 4 * (size_t)cnt);
+  } else if (p) {
+    *p = q;
+  }
+  if (flags) *flags = fl;
+  *n = cnt;
+  return NB_OK;
+}
+
 int nb_write_frame(const char* dir, int index, int n, const float* pos4) {
   if (!dir || !pos4 || n <= 0 || index < 0) return set_error(NB_ERR_INVALID, "bad argument");
   char name[64];

@@ -469,6 +469,7 @@ struct LevelArgs {
   const void* keys;                 // first level
   const float4* __restrict__ ps;
   Node* nodes;
+  PairRec* pairs;                   // child pairs by split, or nullptr
   int* parent;
   double4* sums;
   float4* box_lo;
@@ -497,6 +498,7 @@ struct TreeView {
   int base;             // first slot of this tree in the arrays of p
   __device__ const float4* ps() const { return p.ps + base; }
   __device__ Node* nodes() const { return p.nodes + base; }
+  __device__ PairRec* pairs() const { return p.pairs ? p.pairs + base : nullptr; }
   __device__ int* parent() const { return p.parent + 2 * (size_t)base; }
   __device__ double4* sums() const { return p.sums + base; }
   __device__ float4* box_lo() const { return p.box_lo + base; }
@@ -539,8 +541,32 @@ __device__ __forceinline__ Cell merge(const Cell& a, const Cell& b) {
   return c;
 }
 
+// One child's half of its parent's pair record: the left half (side 0) of
+// record k when the child's parent splits after leaf k and the child covers
+// the leaves up to k, the right half (side 1) when it covers leaf k + 1
+// onwards.  Writes outside the tree's n - 1 records are skipped and flagged.
+__device__ __forceinline__ void write_pair_half(const TreeView& a, int k, int side,
+                                                float4 p, float size2, int w) {
+  PairRec* pr = a.pairs();
+  if (!pr) return;
+  if (k < 0 || k >= a.n - 1) {
+    raise_err(a.err(), NB_DEVERR_BOUNDS);
+    return;
+  }
+  float* r = reinterpret_cast<float*>(&pr[k]);
+  r[side] = p.x;
+  r[2 + side] = p.y;
+  r[4 + side] = p.z;
+  r[6 + side] = p.w;
+  r[8 + side] = size2;
+  r[10 + side] = __int_as_float(w);
+}
+
 // Node record of internal node id over leaves [lo, hi] split after leaf sc,
-// and the parent links of its two children.
+// the parent links of its two children and its half of its parent's pair
+// record.  A non-root internal node's Karras id is hi when it is its
+// parent's left child (its parent splits after leaf hi) and lo when it is
+// the right child (its parent splits after leaf lo - 1).
 __device__ __forceinline__ void write_node(const TreeView& a, int id, int lo,
                                            int hi, int sc, const Cell& c) {
   const int ni = a.n - 1;
@@ -557,11 +583,16 @@ __device__ __forceinline__ void write_node(const TreeView& a, int id, int lo,
   com.w = __double2float_rn(c.s.w);
   const float e = fmaxf(__fsub_rn(c.hi.x, c.lo.x),
                         fmaxf(__fsub_rn(c.hi.y, c.lo.y), __fsub_rn(c.hi.z, c.lo.z)));
+  const float size2 = __fmul_rn(e, e);
   float4* rec = reinterpret_cast<float4*>(&a.nodes()[id]);
   rec[0] = com;
-  reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(__fmul_rn(e, e)), 0);
+  reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(size2), 0);
   a.parent()[l] = id;
   a.parent()[r] = id;
+  if (!(lo == 0 && hi == ni)) {
+    if (id == hi) write_pair_half(a, id, 0, com, size2, sc);
+    else write_pair_half(a, id - 1, 1, com, size2, sc);
+  }
 }
 
 __device__ __forceinline__ void store_cell(const TreeView& a, int id, const Cell& c) {
@@ -806,6 +837,10 @@ __global__ void __launch_bounds__(kLevelThreads, 2) k_build_level(LevelArgs args
       Cell c;
       if (FIRST || lo == hi) {
         c = leaf_cell(a.ps(), lo);
+        if (FIRST && ni > 0) {   // the leaf's half of its parent's pair record
+          const bool right = lo == 0 || (hi != ni && sm.delta[j + 1] > sm.delta[j]);
+          write_pair_half(a, right ? lo : lo - 1, right ? 0 : 1, a.ps()[lo], -1.f, -1);
+        }
       } else {   // a subtree finished below: its Karras id follows its direction
         const bool right = lo == 0 || (hi != ni && sm.delta[j + 1] > sm.delta[j]);
         const int kid = right ? hi : lo;
@@ -926,6 +961,7 @@ static LevelArgs level_args(Workspace& w, const StepArgs& a) {
   b.keys = w.keys;
   b.ps = w.pos_sorted;
   b.nodes = w.nodes;
+  b.pairs = w.pairs;
   b.parent = w.parent;
   b.sums = w.sums;
   b.box_lo = w.box_lo;
@@ -1131,6 +1167,7 @@ int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st) 
   b.keys = e.keys;
   b.ps = e.pos_sorted;
   b.nodes = e.nodes;
+  b.pairs = e.pairs;
   b.parent = e.parent;
   b.sums = e.sums;
   b.box_lo = e.box_lo;

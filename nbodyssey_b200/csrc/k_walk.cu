@@ -80,6 +80,7 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
   a.ps = w.pos_sorted;
   a.perm = w.vals;
   a.nodes = w.nodes;
+  a.pairs = w.pairs;
   a.theta2 = s.theta2;
   a.eps2 = s.eps2;
   a.G = s.G;
@@ -93,6 +94,8 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
   a.t1 = s.t1;
   a.part = s.part;
   if (s.walk_kernel == 0)
+    return launch_walk_pair(a, s.traverse == NB_TRAVERSE_THREAD, st);
+  if (s.walk_kernel == 2)
     return launch_walk_list(a, s.traverse == NB_TRAVERSE_THREAD, st);
   int blocks = (s.t1 - s.t0 + 255) / 256;
   if (blocks == 0) return NB_OK;

@@ -377,48 +377,6 @@ __global__ void __launch_bounds__(kLW * 32) k_walk_list(WalkArgs a) {
   walk_list_warp<MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * kLW + (threadIdx.x >> 5), sm);
 }
 
-// Ensemble: each warp takes one 32-slot block of the concatenated sorted
-// arrays; blocks belong to one simulation (bases are multiples of 32), whose
-// tree, parameters and semantics the walk uses.  Simulations with the other
-// semantics are left to the other instantiation.
-template <bool MASKED>
-__global__ void __launch_bounds__(kLW * 32) k_walk_list_ens(EnsArgs e) {
-  __shared__ ListSmem<MASKED> sm;
-  const int blk = blockIdx.x * kLW + (threadIdx.x >> 5);
-  if (blk >= e.nblocks) return;
-  const int s = e.blk_sim[blk];
-  if (s < 0) return;
-  const SimDesc d = e.sims[s];
-  if (!d.active || d.n < 2 || (d.traverse == NB_TRAVERSE_THREAD) != MASKED) return;
-  WalkArgs a;
-  a.n = d.n;
-  a.ps = e.pos_sorted + d.base;
-  a.perm = e.perm + d.base;
-  a.nodes = e.nodes + d.base;
-  a.theta2 = d.theta2;
-  a.eps2 = d.eps2;
-  a.G = d.G;
-  a.half_dt = d.half_dt;
-  a.acc = e.acc;
-  a.vel = (e.kick_after && d.active == 1) ? e.vel : nullptr;
-  a.counts = nullptr;
-  a.perm_limit = e.nslots;
-  a.err = e.err;
-  a.t0 = 0;
-  a.t1 = d.n;
-  a.part = nullptr;
-  walk_list_warp<MASKED, false, true>(a, blk - d.base / 32, sm);
-}
-
-int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
-  const int blocks = (e.nblocks + kLW - 1) / kLW;
-  if (blocks == 0) return NB_OK;
-  k_walk_list_ens<false><<<blocks, kLW * 32, 0, st>>>(e);
-  k_walk_list_ens<true><<<blocks, kLW * 32, 0, st>>>(e);
-  NB_CUDA(cudaGetLastError());
-  return NB_OK;
-}
-
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st) {
   const int warps = (a.t1 - a.t0 + 31) / 32;
   if (warps <= 0) return NB_OK;

@@ -1,0 +1,456 @@
+// Default Barnes-Hut walk (walk_kernel = 0): the reference's interaction sets
+// (src/forces_bh.cu:335-447) computed from the tree's child-pair records.
+//
+// A warp owns 32 consecutive Morton-sorted targets and keeps a stack of
+// opened internal nodes in shared memory, each as the split whose pair record
+// (PairRec, nb_internal.cuh) holds its two children.  Each warp step takes up
+// to 32 opened nodes, one per lane, and every lane decides both children of
+// its node from one 48-byte record fetch:
+//
+// * a leaf (size2 = -1) is accepted by every test: it becomes an
+//   interaction-list entry;
+// * an internal child is accepted by every target when even the nearest point
+//   of the box of the 32 targets accepts it (size2 < theta2 * dmin2 with a
+//   1e-5 relative margin, far above the few-ulp rounding of the exact test);
+// * warp semantics: otherwise the group's extreme target along the child's
+//   dominant direction is tested exactly, and its rejection opens the child
+//   (a farthest-box-point rejection implies it, so that test is not needed);
+// * thread semantics: a child that even the farthest box point rejects is
+//   rejected by every target;
+// * the children still undecided are staged in shared memory and every lane
+//   tests its own target against two of them per packed instruction, in the
+//   float order of accepts() (walk_common.cuh), so every decision equals the
+//   per-target float test bit for bit.
+//
+// Warp semantics (traverse = warp, src/forces_bh.cu:395-447): a child opens
+// when any live target rejects it, otherwise all targets take it.  Thread
+// semantics (traverse = thread, src/forces_bh.cu:335-377): each opened node
+// carries the mask of the targets whose own walk opened it; the targets that
+// accept a child take it (an entry with their mask) and the others pass it on
+// opened.  Either way every target gets exactly the reference's set.
+//
+// Entries go to a 128-entry ring per warp (pairs interleaved as
+// (x0,x1,y0,y1)(z0,z1,m0,m1)), evaluated 32 at a time by an unrolled body
+// with packed FP32 math, two entries per instruction; entries whose mask
+// excludes a lane contribute with mass 0.  A stack that would overflow hands
+// the warp to the depth-first walk of the same semantics.
+#include "f32x2.cuh"
+#include "walk_common.cuh"
+
+namespace nb {
+
+constexpr int kPW = 4;            // warps per block
+constexpr int kPStack = 512;      // opened-node entries per warp
+constexpr int kPRing = 128;       // interaction-list ring entries per warp
+constexpr int kPFlush = 32;       // entries evaluated per flush
+constexpr int kPAmb = 64;         // children staged for the all-target test
+
+template <bool MASKED>
+struct PairSmem {
+  int stk[kPW][kPStack];
+  unsigned smask[kPW][MASKED ? kPStack : 1];
+  __align__(16) float ent[kPW][kPRing * 4];
+  unsigned emask[kPW][MASKED ? kPRing : 1];
+  __align__(16) float amb[kPW][kPAmb * 4];
+  unsigned res[kPW][kPAmb];
+  float4 ext[kPW][MASKED ? 1 : 6];
+};
+
+__device__ __forceinline__ float pw_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ float pw_max(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// (v, v) in one register pair, made at each use (volatile: not hoisted and
+// kept live through the walk)
+__device__ __forceinline__ f2 pk2u(float v) {
+  f2 r;
+  asm volatile("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(v));
+  return r;
+}
+
+// Writes one list entry (x, y, z, m) at ring position k.
+__device__ __forceinline__ void put_entry(float* ent, int k, float x, float y,
+                                          float z, float m) {
+  k &= kPRing - 1;
+  float* p = &ent[(k >> 1) * 8 + (k & 1)];
+  p[0] = x;
+  p[2] = y;
+  p[4] = z;
+  p[6] = m;
+}
+
+// Squared distance from (cx, cy, cz) to the nearest / farthest point of the
+// box [lo, hi] (rounded; the callers' margins cover it).
+__device__ __forceinline__ float box_near2(float cx, float cy, float cz, float lox,
+                                           float loy, float loz, float hix,
+                                           float hiy, float hiz) {
+  const float ex = fmaxf(fmaxf(lox - cx, cx - hix), 0.f);
+  const float ey = fmaxf(fmaxf(loy - cy, cy - hiy), 0.f);
+  const float ez = fmaxf(fmaxf(loz - cz, cz - hiz), 0.f);
+  return ex * ex + ey * ey + ez * ez;
+}
+__device__ __forceinline__ float box_far2(float cx, float cy, float cz, float lox,
+                                          float loy, float loz, float hix,
+                                          float hiy, float hiz) {
+  const float fx = fmaxf(fabsf(lox - cx), fabsf(cx - hix));
+  const float fy = fmaxf(fabsf(loy - cy), fabsf(cy - hiy));
+  const float fz = fmaxf(fabsf(loz - cz), fabsf(cz - hiz));
+  return fx * fx + fy * fy + fz * fz;
+}
+
+// The walk of warp `wg` (targets 32wg .. 32wg+31); all 32 lanes call it.
+template <bool MASKED, bool COUNT, bool HOIST = false>
+__device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
+                                               PairSmem<MASKED>& sm) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int n = a.n, ni = n - 1;
+  if (wg * 32 >= a.t1) return;   // whole warp past the end of the range
+  const int t = wg * 32 + lane;
+  const bool live = t < n;
+  const unsigned live_mask = __ballot_sync(full, live);
+  const unsigned lt = (1u << lane) - 1u;
+  // dead lanes (last warp only) copy particle n-1, a live lane of this warp,
+  // so the group box is the box of the live targets and a dead lane's exact
+  // tests repeat a live lane's
+  const float4 bi = a.ps[live ? t : n - 1];
+  const float lox = pw_min(bi.x), loy = pw_min(bi.y), loz = pw_min(bi.z);
+  const float hix = pw_max(bi.x), hiy = pw_max(bi.y), hiz = pw_max(bi.z);
+  const float theta2 = a.theta2;
+  const float th_lo = theta2 * 0.99999f, th_hi = theta2 * 1.00001f;
+  if (!MASKED) {
+    // the targets at the group's extremes (warp semantics: one rejecting
+    // target opens a child for all)
+    const float lv[6] = {lox, hix, loy, hiy, loz, hiz};
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const float c = (e < 2) ? bi.x : (e < 4 ? bi.y : bi.z);
+      const int src = __ffs(__ballot_sync(full, c == lv[e])) - 1;
+      const float ex = __shfl_sync(full, bi.x, src), ey = __shfl_sync(full, bi.y, src),
+                  ez = __shfl_sync(full, bi.z, src);
+      if (lane == 0) sm.ext[w][e] = make_float4(ex, ey, ez, 0.f);
+    }
+  }
+  const float cmx = 0.5f * (lox + hix), cmy = 0.5f * (loy + hiy), cmz = 0.5f * (loz + hiz);
+
+  const float mx = -bi.x, my = -bi.y, mz = -bi.z;   // this lane's target, negated
+  const f2 hx = pk2(mx, mx), hy = pk2(my, my), hz = pk2(mz, mz), he2 = pk2(a.eps2, a.eps2);
+  auto px = [&]() { return HOIST ? hx : pk2u(mx); };
+  auto py = [&]() { return HOIST ? hy : pk2u(my); };
+  auto pz = [&]() { return HOIST ? hz : pk2u(mz); };
+  f2 ax = 0ull, ay = 0ull, az = 0ull;
+  int cnt = 0;
+  float* ent = sm.ent[w];
+  int head = 0;   // ring position of the first unevaluated entry (multiple of 32)
+  int lc = 0;     // unevaluated entries
+
+  // list pair q of the 32-entry block at ring position `at`
+  auto pair_term = [&](int at, int q) {
+    const float* base = &ent[at * 4];
+    const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&base[q * 8]);
+    const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&base[q * 8 + 4]);
+    f2 m = B.y;
+    if (MASKED) {
+      const unsigned b0 = (sm.emask[w][at + 2 * q] >> lane) & 1u;
+      const unsigned b1 = (sm.emask[w][at + 2 * q + 1] >> lane) & 1u;
+      float m0, m1;
+      up2(B.y, m0, m1);
+      m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
+      if (COUNT) cnt += (int)(b0 + b1);
+    }
+    f2 dx = add2(A.x, px());
+    f2 dy = add2(A.y, py());
+    f2 dz = add2(B.x, pz());
+    f2 r2 = fma2(dz, dz, HOIST ? he2 : pk2u(a.eps2));
+    r2 = fma2(dy, dy, r2);
+    r2 = fma2(dx, dx, r2);
+    float r0, r1;
+    up2(r2, r0, r1);
+    f2 inv = pk2(mufu_rsqrt(r0), mufu_rsqrt(r1));
+    f2 wm = mul2(inv, m);
+    f2 i2 = mul2(inv, inv);
+    f2 f = mul2(wm, i2);
+    ax = fma2(dx, f, ax);
+    ay = fma2(dy, f, ay);
+    az = fma2(dz, f, az);
+  };
+  // evaluates the 32 entries at `head` (unrolled, fixed offsets)
+  auto flush_full = [&]() {
+#pragma unroll
+    for (int q = 0; q < kPFlush / 2; ++q) pair_term(head, q);
+    if (!MASKED && COUNT) cnt += kPFlush;
+    head = (head + kPFlush) & (kPRing - 1);
+    lc -= kPFlush;
+  };
+
+  // the root: one exact test per target (dead lanes repeat a live one)
+  int sp = 0;
+  {
+    const Node root = a.nodes[0];
+    const bool acc = accepts(root.size2, theta2, root.com.x, root.com.y, root.com.z,
+                             bi.x, bi.y, bi.z);
+    const int sc0 = root.left < ni ? root.left : root.left - ni;
+    const unsigned am = MASKED ? (__ballot_sync(full, acc) & live_mask)
+                               : (__all_sync(full, acc) ? live_mask : 0u);
+    if (lane == 0) {
+      if (am) {
+        put_entry(ent, 0, root.com.x, root.com.y, root.com.z, root.com.w);
+        if (MASKED) sm.emask[w][0] = am;
+      }
+      if (am != live_mask) {
+        sm.stk[w][0] = sc0;
+        if (MASKED) sm.smask[w][0] = live_mask & ~am;
+      }
+    }
+    lc = am ? 1 : 0;
+    sp = am != live_mask ? 1 : 0;
+    __syncwarp();
+  }
+
+  bool overflow = false;
+  for (int guard = 0; sp > 0; ++guard) {
+    if (sp + 32 > kPStack || guard > n) {   // uniform across the warp
+      overflow = true;
+      break;
+    }
+    const int take = min(sp, 32);
+    const int base = sp - take;
+    const bool has = lane < take;
+    int k = 0;
+    unsigned M = live_mask;
+    if (has) {
+      k = sm.stk[w][base + lane];
+      if (MASKED) M = sm.smask[w][base + lane];
+    }
+    __syncwarp();
+    sp = base;
+    k = min(max(k, 0), ni - 1);   // a valid tree never needs the clamp
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
+    if (has) {
+      const PairRec* r = a.pairs + k;
+      A = r->a;
+      B = r->b;
+      C = r->c;
+    }
+    // child 0 = (A.x, A.z, B.x) mass B.z size2 C.x split C.z; child 1 = .y/.w
+    const int w0 = __float_as_int(C.z), w1 = __float_as_int(C.w);
+    const f2 dn = pk2(box_near2(A.x, A.z, B.x, lox, loy, loz, hix, hiy, hiz),
+                      box_near2(A.y, A.w, B.y, lox, loy, loz, hix, hiy, hiz));
+    float tn0, tn1;
+    up2(mul2(pk2u(th_lo), dn), tn0, tn1);
+    const bool bacc0 = C.x < tn0, bacc1 = C.y < tn1;   // leaves: -1 < anything >= 0
+    bool amb0, amb1, brej0 = false, brej1 = false;
+    if (MASKED) {
+      const f2 df = pk2(box_far2(A.x, A.z, B.x, lox, loy, loz, hix, hiy, hiz),
+                        box_far2(A.y, A.w, B.y, lox, loy, loz, hix, hiy, hiz));
+      float tf0, tf1;
+      up2(mul2(pk2u(th_hi), df), tf0, tf1);
+      brej0 = !bacc0 && C.x > tf0;
+      brej1 = !bacc1 && C.y > tf1;
+      amb0 = has && !bacc0 && !brej0;
+      amb1 = has && !bacc1 && !brej1;
+    } else {
+      // the group's extreme target along the child's dominant direction
+      // from the box centre; its exact rejection opens the child
+      auto ext_accepts = [&](float s2, float cx, float cy, float cz) {
+        const float rx = cx - cmx, ry = cy - cmy, rz = cz - cmz;
+        const float qx = fabsf(rx), qy = fabsf(ry), qz = fabsf(rz);
+        const int e = (qx >= qy && qx >= qz) ? (rx > 0.f ? 1 : 0)
+                                             : (qy >= qz ? (ry > 0.f ? 3 : 2) : (rz > 0.f ? 5 : 4));
+        const float4 q = sm.ext[w][e];
+        return accepts(s2, theta2, cx, cy, cz, q.x, q.y, q.z);
+      };
+      amb0 = has && !bacc0 && ext_accepts(C.x, A.x, A.z, B.x);
+      amb1 = has && !bacc1 && ext_accepts(C.y, A.y, A.w, B.y);
+    }
+    // children the box and the extreme target cannot settle: staged in
+    // shared memory (pairs interleaved as (cx0,cx1,cy0,cy1)(cz0,cz1,s0,s1));
+    // every lane tests its own target against two per packed instruction, in
+    // the float order of accepts(), and one ballot per child is written back
+    unsigned r0 = 0u, r1 = 0u;
+    const unsigned ab0 = __ballot_sync(full, amb0), ab1 = __ballot_sync(full, amb1);
+    if (ab0 | ab1) {
+      const int na0 = __popc(ab0), na = na0 + __popc(ab1);
+      const int ka0 = __popc(ab0 & lt), ka1 = na0 + __popc(ab1 & lt);
+      float* am = sm.amb[w];
+      if (amb0) {
+        float* p = &am[(ka0 >> 1) * 8 + (ka0 & 1)];
+        p[0] = A.x; p[2] = A.z; p[4] = B.x; p[6] = C.x;
+      }
+      if (amb1) {
+        float* p = &am[(ka1 >> 1) * 8 + (ka1 & 1)];
+        p[0] = A.y; p[2] = A.w; p[4] = B.y; p[6] = C.y;
+      }
+      if ((na & 1) && lane == 0) {   // pad: a child every target accepts
+        float* p = &am[(na >> 1) * 8 + 1];
+        p[0] = 0.f; p[2] = 0.f; p[4] = 0.f; p[6] = -1.f;
+      }
+      __syncwarp();
+      const f2 th2 = pk2(theta2, theta2);
+      for (int q = 0; q < (na + 1) >> 1; ++q) {
+        const ulonglong2 U = *reinterpret_cast<const ulonglong2*>(&am[q * 8]);
+        const ulonglong2 V = *reinterpret_cast<const ulonglong2*>(&am[q * 8 + 4]);
+        const f2 dx = add2(U.x, px()), dy = add2(U.y, py()), dz = add2(V.x, pz());
+        const f2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+        float t0, t1, z0, z1;
+        up2(mul2(th2, d2), t0, t1);
+        up2(V.y, z0, z1);
+        const unsigned v0 = __ballot_sync(full, z0 < t0);
+        const unsigned v1 = __ballot_sync(full, z1 < t1);
+        if (lane == 0) {
+          sm.res[w][2 * q] = v0;
+          sm.res[w][2 * q + 1] = v1;
+        }
+      }
+      __syncwarp();
+      if (amb0) r0 = sm.res[w][ka0];
+      if (amb1) r1 = sm.res[w][ka1];
+    }
+    // accepting targets of each child
+    unsigned acc0, acc1;
+    if (MASKED) {
+      acc0 = bacc0 ? M : (amb0 ? (r0 & M) : 0u);
+      acc1 = bacc1 ? M : (amb1 ? (r1 & M) : 0u);
+    } else {
+      acc0 = (bacc0 || (amb0 && (r0 & live_mask) == live_mask)) ? M : 0u;
+      acc1 = (bacc1 || (amb1 && (r1 & live_mask) == live_mask)) ? M : 0u;
+    }
+    const bool ent0 = has && acc0 != 0u, ent1 = has && acc1 != 0u;
+    const bool psh0 = has && acc0 != M && w0 >= 0, psh1 = has && acc1 != M && w1 >= 0;
+    const unsigned eb0 = __ballot_sync(full, ent0), eb1 = __ballot_sync(full, ent1);
+    const int ne0 = __popc(eb0);
+    if (ent0) {
+      const int e = head + lc + __popc(eb0 & lt);
+      put_entry(ent, e, A.x, A.z, B.x, B.z);
+      if (MASKED) sm.emask[w][e & (kPRing - 1)] = acc0;
+    }
+    if (ent1) {
+      const int e = head + lc + ne0 + __popc(eb1 & lt);
+      put_entry(ent, e, A.y, A.w, B.y, B.w);
+      if (MASKED) sm.emask[w][e & (kPRing - 1)] = acc1;
+    }
+    lc += ne0 + __popc(eb1);
+    const unsigned pb0 = __ballot_sync(full, psh0), pb1 = __ballot_sync(full, psh1);
+    const int np0 = __popc(pb0);
+    if (psh0) {
+      const int s = sp + __popc(pb0 & lt);
+      sm.stk[w][s] = w0;
+      if (MASKED) sm.smask[w][s] = M & ~acc0;
+    }
+    if (psh1) {
+      const int s = sp + np0 + __popc(pb1 & lt);
+      sm.stk[w][s] = w1;
+      if (MASKED) sm.smask[w][s] = M & ~acc1;
+    }
+    sp += np0 + __popc(pb1);
+    __syncwarp();
+    while (lc >= kPFlush) flush_full();
+    __syncwarp();
+  }
+
+  float3 ai;
+  if (!overflow) {
+    if (lc) {   // the last, partial block (lc < 32, contiguous at head)
+      if (lc & 1) {   // pad to a whole pair with a zero-mass entry
+        if (lane == 0) {
+          put_entry(ent, head + lc, 0.f, 0.f, 0.f, 0.f);
+          if (MASKED) sm.emask[w][(head + lc) & (kPRing - 1)] = 0u;
+        }
+        __syncwarp();
+      }
+      const int np = (lc + 1) >> 1;
+      for (int q = 0; q < np; ++q) pair_term(head, q);
+      if (!MASKED && COUNT) cnt += lc;
+    }
+    float u, v;
+    up2(ax, u, v); ai.x = u + v;
+    up2(ay, u, v); ai.y = u + v;
+    up2(az, u, v); ai.z = u + v;
+  } else {
+    // same interaction set by the depth-first walk; the stack's shared
+    // memory serves as the warp stack
+    cnt = 0;
+    __syncwarp();
+    if (MASKED)
+      ai = dfs_walk_thread<COUNT>(a, bi, &cnt);
+    else
+      ai = dfs_walk_warp<COUNT>(a, bi, live, sm.stk[w], &cnt);
+  }
+  if (live) {
+    epilogue(a, t, ai);
+    if (COUNT) a.counts[t] = cnt;
+  }
+}
+
+template <bool MASKED, bool COUNT>
+__global__ void __launch_bounds__(kPW * 32) k_walk_pair(WalkArgs a) {
+  __shared__ PairSmem<MASKED> sm;
+  walk_pair_warp<MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * kPW + (threadIdx.x >> 5), sm);
+}
+
+// Ensemble: each warp takes one 32-slot block of the concatenated sorted
+// arrays; blocks belong to one simulation (bases are multiples of 32), whose
+// tree, parameters and semantics the walk uses.  Simulations with the other
+// semantics are left to the other instantiation.
+template <bool MASKED>
+__global__ void __launch_bounds__(kPW * 32) k_walk_pair_ens(EnsArgs e) {
+  __shared__ PairSmem<MASKED> sm;
+  const int blk = blockIdx.x * kPW + (threadIdx.x >> 5);
+  if (blk >= e.nblocks) return;
+  const int s = e.blk_sim[blk];
+  if (s < 0) return;
+  const SimDesc d = e.sims[s];
+  if (!d.active || d.n < 2 || (d.traverse == NB_TRAVERSE_THREAD) != MASKED) return;
+  WalkArgs a;
+  a.n = d.n;
+  a.ps = e.pos_sorted + d.base;
+  a.perm = e.perm + d.base;
+  a.nodes = e.nodes + d.base;
+  a.pairs = e.pairs + d.base;
+  a.theta2 = d.theta2;
+  a.eps2 = d.eps2;
+  a.G = d.G;
+  a.half_dt = d.half_dt;
+  a.acc = e.acc;
+  a.vel = (e.kick_after && d.active == 1) ? e.vel : nullptr;
+  a.counts = nullptr;
+  a.perm_limit = e.nslots;
+  a.err = e.err;
+  a.t0 = 0;
+  a.t1 = d.n;
+  a.part = nullptr;
+  walk_pair_warp<MASKED, false, true>(a, blk - d.base / 32, sm);
+}
+
+int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
+  const int blocks = (e.nblocks + kPW - 1) / kPW;
+  if (blocks == 0) return NB_OK;
+  k_walk_pair_ens<false><<<blocks, kPW * 32, 0, st>>>(e);
+  k_walk_pair_ens<true><<<blocks, kPW * 32, 0, st>>>(e);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
+  const int warps = (a.t1 - a.t0 + 31) / 32;
+  if (warps <= 0) return NB_OK;
+  const int blocks = (warps + kPW - 1) / kPW;
+  if (masked) {
+    if (a.counts) k_walk_pair<true, true><<<blocks, kPW * 32, 0, st>>>(a);
+    else k_walk_pair<true, false><<<blocks, kPW * 32, 0, st>>>(a);
+  } else {
+    if (a.counts) k_walk_pair<false, true><<<blocks, kPW * 32, 0, st>>>(a);
+    else k_walk_pair<false, false><<<blocks, kPW * 32, 0, st>>>(a);
+  }
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+}  // namespace nb

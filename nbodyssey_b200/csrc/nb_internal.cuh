@@ -44,6 +44,21 @@ struct __align__(16) Node {
   int pad;
 };
 
+// Child pairs for the tree walk, one record per split k in [0, n-2]: the two
+// children of the internal node that splits its leaves after leaf k (the left
+// child is internal node k or leaf k, the right child internal node k+1 or
+// leaf k+1), interleaved so that one lane's three 16-byte loads give packed
+// pairs: a = (x_l, x_r, y_l, y_r), b = (z_l, z_r, m_l, m_r),
+// c = (size2_l, size2_r, w_l, w_r) with (x, y, z, m) the centre of mass and
+// mass of an internal child or the position and mass of a leaf, size2 the
+// squared longest edge of an internal child's box (-1 for a leaf, which every
+// opening test accepts) and w the split of an internal child, where its own
+// children are recorded (-1 for a leaf).  The tree build writes each child's
+// half of its parent's record; the root is the one node with no record.
+struct __align__(16) PairRec {
+  float4 a, b, c;
+};
+
 // Walks keep their per-warp / per-thread stacks this deep.  A radix tree over
 // 63-bit keys with index tie-breaks is at most 63 + 31 levels deep and the
 // stack grows by at most one entry per level; an overflow raises
@@ -81,6 +96,7 @@ struct Workspace {
   uint32_t* vals_alt = nullptr;
   float4* pos_sorted = nullptr;   // [cap]
   Node* nodes = nullptr;          // [cap-1]
+  PairRec* pairs = nullptr;       // [cap-1] child pairs by split
   int* parent = nullptr;          // [2cap-1]
   int2* seg[2] = {nullptr, nullptr};      // open splits per build CTA,
   int* seg_count[2] = {nullptr, nullptr}; // ping-pong between levels
@@ -241,6 +257,7 @@ struct EnsArgs {
   uint32_t* perm;             // [nslots] x2: original slot of each sorted slot
   uint32_t* perm_alt;
   Node* nodes;                // [nslots]
+  PairRec* pairs;             // [nslots] child pairs by split
   int* parent;                // [2 nslots]
   double4* sums;              // [nslots]
   float4* box_lo;

@@ -35,8 +35,9 @@ using namespace nb;
 
 namespace {
 
-constexpr size_t kBytesPerSlot = 224;   // state 64, sorted 16, keys 16, perm 8,
-                                        // nodes 32, parent 8, sums 32, boxes 32,
+constexpr size_t kBytesPerSlot = 272;   // state 64, sorted 16, keys 16, perm 8,
+                                        // nodes 32, child pairs 48, parent 8,
+                                        // sums 32, boxes 32,
                                         // sort scratch ~12, build plan and
                                         // segments ~4
 constexpr int kInFlight = 2;            // engine steps queued ahead of the GPU
@@ -437,6 +438,7 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     if ((rc = srv_alloc(s, &e.perm, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.perm_alt, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.nodes, S)) != NB_OK) break;
+    if ((rc = srv_alloc(s, &e.pairs, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.parent, 2 * S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.sums, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.box_lo, S)) != NB_OK) break;
@@ -481,6 +483,7 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     if (ce == cudaSuccess) ce = cudaMemset(e.perm, 0, S * 4);
     if (ce == cudaSuccess) ce = cudaMemset(e.perm_alt, 0, S * 4);
     if (ce == cudaSuccess) ce = cudaMemset(e.nodes, 0, S * sizeof(Node));
+    if (ce == cudaSuccess) ce = cudaMemset(e.pairs, 0, S * sizeof(PairRec));
     if (ce == cudaSuccess) ce = cudaMemset(e.hist, 0, words * 4);
     if (ce == cudaSuccess) ce = cudaMemset(e.err, 0, 16);
     if (ce == cudaSuccess) ce = cudaMemset(dblk, 0xff, S / 32 * sizeof(int));

@@ -16,6 +16,7 @@ struct WalkArgs {
   const float4* __restrict__ ps;      // sorted positions
   const uint32_t* __restrict__ perm;  // sorted -> original
   const Node* __restrict__ nodes;
+  const PairRec* __restrict__ pairs;  // child pairs by split (pair walk)
   float theta2, eps2, G, half_dt;
   float4* acc;       // original order
   float4* vel;       // closing kick target (original order) or nullptr
@@ -176,6 +177,7 @@ __device__ __forceinline__ float3 dfs_walk_warp(const WalkArgs& a, float4 bi,
 }
 
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st);
+int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st);
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
 
 }  // namespace nb

@@ -8,9 +8,12 @@
 Flags and defaults follow src/main.cu:18-70 (dt 0.01, eps 0.05, G 1, theta
 0.5, naive, thread, 1000 steps, a frame + energy row every 5 steps, frames to
 ./frames, energy log benchmarks/energy_gpu.csv).  Extra flags: --key-bits
-(30|63), --plain-drift (no hi/lo compensation), --walk (list|dfs).  The run
-loop itself is native (nb_run): frames stream out asynchronously while the
-next steps run.
+(30|63), --plain-drift (no hi/lo compensation), --walk (pair|list|dfs),
+--checkpoint PATH (a state file of the final state: the ic.bin layout plus a
+trailer with the parameters, the low-order position parts and a(x)) and
+--resume PATH (continue from such a file, with its parameters, bit for bit as
+if the run had not stopped; --ic is then not needed).  The run loop itself is
+native (nb_run): frames stream out asynchronously while the next steps run.
 """
 from __future__ import annotations
 
@@ -24,7 +27,7 @@ from . import api, formats
 def parse_args(argv=None):
     ap = argparse.ArgumentParser(prog="galaxy_sim", description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--ic", required=True)
+    ap.add_argument("--ic")
     ap.add_argument("--out", default="frames")
     ap.add_argument("--energy-log", default="benchmarks/energy_gpu.csv")
     ap.add_argument("--steps", type=int, default=1000)
@@ -38,26 +41,33 @@ def parse_args(argv=None):
     ap.add_argument("--compare-forces", action="store_true")
     ap.add_argument("--key-bits", type=int, choices=[30, 63], default=30)
     ap.add_argument("--plain-drift", action="store_true")
-    ap.add_argument("--walk", choices=["list", "dfs"], default="list")
-    return ap.parse_args(argv)
+    ap.add_argument("--walk", choices=["pair", "list", "dfs"], default="pair")
+    ap.add_argument("--checkpoint", help="write the final state to this state file")
+    ap.add_argument("--resume", help="start from this state file instead of --ic")
+    a = ap.parse_args(argv)
+    if not a.ic and not a.resume:
+        ap.error("one of --ic or --resume is required")
+    return a
 
 
 def main(argv=None):
     a = parse_args(argv)
-    try:
-        pos4, vel4 = formats.read_ic(a.ic)
-    except (OSError, formats.FormatError) as e:
-        print(e, file=sys.stderr)
-        return 1
     params = api.SimParams(dt=a.dt, epsilon=a.eps, G=a.G, theta=a.theta,
                            force=a.force, traverse=a.traverse, key_bits=a.key_bits,
                            compensated=not a.plain_drift, walk_kernel=a.walk)
-    n = pos4.shape[0]
     try:
-        sim = api.Simulation(pos4, vel4, params)
-    except L.NbError as e:
+        if a.resume:
+            sim = api.Simulation.from_state(a.resume)
+            params = sim.params
+            a.dt, a.eps, a.theta = params.dt, params.epsilon, params.theta
+            a.force, a.traverse = params.force, params.traverse
+        else:
+            pos4, vel4 = formats.read_ic(a.ic)
+            sim = api.Simulation(pos4, vel4, params)
+    except (OSError, formats.FormatError, L.NbError) as e:
         print(e, file=sys.stderr)
         return 1
+    n = sim.n
     with sim:
         if a.compare_forces:
             # src/main.cu:75-112; gpu_bench.sh greps the second line
@@ -89,6 +99,9 @@ def main(argv=None):
             print("throughput: %.2f Ginteractions/s (~%.1f GFLOP/s at 20 flop/pair)" %
                   (gips, gips * 20.0))
         print("wrote %d frames to %s" % (st["frames"], a.out))
+        if a.checkpoint:
+            sim.save_state(a.checkpoint)
+            print("wrote state to %s" % a.checkpoint)
     return 0
 
 

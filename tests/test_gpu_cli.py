@@ -57,3 +57,26 @@ def test_bad_ic_is_an_error(tmp_path):
     bad.write_bytes(b"\x05\x00\x00\x00" + b"\x00" * 40)
     r = _run(["--ic", str(bad)], tmp_path)
     assert r.returncode != 0 and "truncated" in r.stderr
+
+
+def test_checkpoint_and_resume(tmp_path):
+    """--checkpoint after 20 steps, --resume for 20 more: the final state
+    equals 40 uninterrupted steps bit for bit."""
+    pos, vel = ic.two_disks(3000, seed=42)
+    icp = tmp_path / "ic.bin"
+    formats.write_ic(str(icp), pos, vel)
+    common = ["--dump-every", "20", "--dt", "0.005", "--force", "bh", "--traverse", "warp",
+              "--energy-log", str(tmp_path / "e.csv")]
+    r = _run(["--ic", str(icp), "--steps", "40", "--out", str(tmp_path / "a"),
+              "--checkpoint", str(tmp_path / "full.bin")] + common, tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = _run(["--ic", str(icp), "--steps", "20", "--out", str(tmp_path / "b"),
+              "--checkpoint", str(tmp_path / "half.bin")] + common, tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = _run(["--resume", str(tmp_path / "half.bin"), "--steps", "20",
+              "--out", str(tmp_path / "c"), "--checkpoint", str(tmp_path / "end.bin"),
+              "--dump-every", "20", "--energy-log", str(tmp_path / "e2.csv")], tmp_path)
+    assert r.returncode == 0, r.stderr
+    a = open(str(tmp_path / "full.bin"), "rb").read()
+    b = open(str(tmp_path / "end.bin"), "rb").read()
+    assert a == b

@@ -33,7 +33,7 @@ def assert_walk_close(acc, ref):
     assert r.max() < 5e-5
 
 
-def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="list"):
+def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="pair"):
     prm = api.SimParams(epsilon=eps, theta=theta, force="bh", traverse=traverse,
                         key_bits=bits, walk_kernel=walk)
     with api.Simulation(pos, np.zeros_like(pos), prm) as sim:
@@ -41,7 +41,7 @@ def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="list"):
     return acc[:, :3].astype(np.float64), cnt.astype(np.int64)
 
 
-@pytest.mark.parametrize("walk", ["list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 @pytest.mark.parametrize("theta", [0.3, 0.5, 0.7])
 @pytest.mark.parametrize("n", [1000, 20_000, 20_001])
@@ -53,7 +53,7 @@ def test_walk_matches_oracle(n, theta, traverse, walk):
     assert_walk_close(acc, ref)
 
 
-@pytest.mark.parametrize("walk", ["list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 def test_walk_matches_oracle_63bit(traverse, walk):
     pos, _ = ic.two_disks(30_000, seed=12)
@@ -63,7 +63,7 @@ def test_walk_matches_oracle_63bit(traverse, walk):
     assert_walk_close(acc, ref)
 
 
-@pytest.mark.parametrize("walk", ["list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 def test_walk_1m_subsample(walk):
     """1M particles, theta 0.5 warp walk: counts of every target equal the
     oracle's (which walks only 4096 sampled warps)."""
@@ -80,7 +80,7 @@ def test_walk_1m_subsample(walk):
     assert_walk_close(acc[orig], ref_w[live])
 
 
-@pytest.mark.parametrize("walk", ["list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 def test_theta0_equals_allpairs(traverse, walk):
     n = 20_000
@@ -211,11 +211,12 @@ def test_list_walk_duplicates_and_clumps(traverse):
             assert_walk_close(acc, ref)
 
 
-def test_list_and_dfs_thread_walks_agree():
-    """The lane-masked list walk gives every target its per-thread
+@pytest.mark.parametrize("walk", ["pair", "list"])
+def test_batched_and_dfs_thread_walks_agree(walk):
+    """The lane-masked batched walks give every target its per-thread
     interaction set: counts equal the one-thread-per-target walk's."""
     pos, _ = ic.two_disks(50_000, seed=17)
-    a1, c1 = bh_forces(pos, 0.5, "thread", walk="list")
+    a1, c1 = bh_forces(pos, 0.5, "thread", walk=walk)
     a2, c2 = bh_forces(pos, 0.5, "thread", walk="dfs")
     assert np.array_equal(c1, c2)
     assert_walk_close(a1, a2.astype(np.float64))
