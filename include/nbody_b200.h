@@ -51,9 +51,9 @@ extern "C" {
  *      BhTraversal) ------------------------------------------------------- */
 #define NB_FORCE_NAIVE 0      /* ForceMethod::kNaive, tiled all-pairs */
 #define NB_FORCE_BH 1         /* ForceMethod::kBarnesHut, LBVH rebuilt per step */
-#define NB_FORCE_AUTO 2       /* all-pairs below NB_AUTO_CROSSOVER particles,
-                                 Barnes-Hut from there on (the per-step times
-                                 cross near 20k particles on a B200) */
+#define NB_FORCE_AUTO 2       /* all-pairs below the tuned crossover, Barnes-Hut
+                                 from there on (nb_tune_table; the default
+                                 NB_AUTO_CROSSOVER is the B200 measurement) */
 #define NB_AUTO_CROSSOVER 20000
 #define NB_TRAVERSE_THREAD 0  /* BhTraversal::kThread, one walk per particle */
 #define NB_TRAVERSE_WARP 1    /* BhTraversal::kWarp, one shared walk per warp */
@@ -92,6 +92,52 @@ NB_API int nb_free_pinned(void* p);
  * all SMs); tflops = 2 * FMAs / time.  Used as the roofline denominator of
  * the FP32-pipe-bound force kernels. */
 NB_API int nb_measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
+
+/* ======================================================================
+ * Autotuning.  No reference counterpart (the reference has one fixed block
+ * size, kForceBlock = 256 in src/forces.cuh:25, and a force module chosen by
+ * hand, src/forces.cu:68-86).  Per device, a table of the all-pairs launch
+ * shape per size, the Barnes-Hut walk's warps per block and the
+ * all-pairs / Barnes-Hut crossover NB_FORCE_AUTO uses, measured on the device
+ * at first use: the first nb_sim_create / nb_ensemble_create /
+ * nb_server_create on a device loads the cache file
+ * ($NBODY_B200_TUNE_CACHE, else ~/.cache/nbodyssey_b200/tune_<device>_<SMs>sm_v1.bin)
+ * or, when there is none, measures the table (about a second) and writes
+ * it.  NBODY_B200_TUNE=off keeps the defaults.  The device-pointer entry
+ * points use the current table and never measure.  The shape decides only
+ * the launch: the same table gives the same bits however it was obtained.
+ * ==================================================================== */
+#define NB_TUNE_VERSION 1
+#define NB_TUNE_BUCKETS 16 /* size bucket b: n < 2^(10+b) (the last: any n) */
+#define NB_TUNE_THETAS 3   /* crossover per theta class 0.3, 0.5, 0.7 */
+typedef struct nb_tune_table {
+  int32_t version;                      /* NB_TUNE_VERSION */
+  int32_t sms;                          /* SMs of the device measured */
+  char device[64];                      /* its name */
+  int32_t ap_threads[NB_TUNE_BUCKETS];  /* all-pairs threads per CTA (128, 256) */
+  int32_t ap_k[NB_TUNE_BUCKETS];        /* targets per thread (2, 4, 8) */
+  int32_t ap_ctas[NB_TUNE_BUCKETS];     /* CTAs wanted in flight (sets the
+                                           source split) */
+  int32_t walk_warps;                   /* Barnes-Hut walk warps per block (2, 4, 8) */
+  int32_t crossover[NB_TUNE_THETAS][2]; /* all-pairs below this many particles,
+                                           per theta class and traversal
+                                           (thread, warp) */
+} nb_tune_table;
+/* Measures the table on the current device and installs it; writes it to
+ * cache_path when non-NULL. */
+NB_API int nb_autotune(const char* cache_path, nb_tune_table* out);
+/* The current device's table (the defaults until one is measured / set). */
+NB_API int nb_tune_get(nb_tune_table* out);
+/* Installs a table for the current device (e.g. a choice made by hand). */
+NB_API int nb_tune_set(const nb_tune_table* t);
+/* The built-in defaults for the current device: 256 x 4 all-pairs shape,
+ * 8 CTAs per SM in flight, 4 walk warps per block, crossover 20,000. */
+NB_API int nb_tune_defaults(nb_tune_table* out);
+/* Loads / saves a cache file (NULL: the default path).  nb_tune_load fails
+ * with NB_ERR_NOTFOUND for a missing file or one measured on another kind of
+ * device. */
+NB_API int nb_tune_load(const char* path);
+NB_API int nb_tune_save(const char* path);
 
 /* ======================================================================
  * Handle API: one simulation whose state lives on the device.

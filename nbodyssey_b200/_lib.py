@@ -54,6 +54,21 @@ class nb_params(ctypes.Structure):
                 ("walk_kernel", ctypes.c_int32)]
 
 
+NB_TUNE_VERSION = 1
+NB_TUNE_BUCKETS = 16
+NB_TUNE_THETAS = 3
+
+
+class nb_tune_table(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_int32), ("sms", ctypes.c_int32),
+                ("device", ctypes.c_char * 64),
+                ("ap_threads", ctypes.c_int32 * NB_TUNE_BUCKETS),
+                ("ap_k", ctypes.c_int32 * NB_TUNE_BUCKETS),
+                ("ap_ctas", ctypes.c_int32 * NB_TUNE_BUCKETS),
+                ("walk_warps", ctypes.c_int32),
+                ("crossover", (ctypes.c_int32 * 2) * NB_TUNE_THETAS)]
+
+
 class nb_run_stats(ctypes.Structure):
     _fields_ = [("wall_s", ctypes.c_double), ("force_ms", ctypes.c_double),
                 ("force_calls", ctypes.c_long), ("frames", ctypes.c_int),
@@ -81,6 +96,12 @@ SIGNATURES = {
     "nb_free_pinned": (_I, [_P]),
     "nb_measure_fp32_peak": (_I, [ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "nb_flush_l2": (_I, [_P, _SZ]),
+    "nb_autotune": (_I, [_S, ctypes.POINTER(nb_tune_table)]),
+    "nb_tune_get": (_I, [ctypes.POINTER(nb_tune_table)]),
+    "nb_tune_set": (_I, [ctypes.POINTER(nb_tune_table)]),
+    "nb_tune_defaults": (_I, [ctypes.POINTER(nb_tune_table)]),
+    "nb_tune_load": (_I, [_S]),
+    "nb_tune_save": (_I, [_S]),
     "nb_sim_create": (_I, [_I, _P, _P, ctypes.POINTER(nb_params), _PP]),
     "nb_sim_destroy": (_I, [_P]),
     "nb_sim_n": (_I, [_P, ctypes.POINTER(_I)]),

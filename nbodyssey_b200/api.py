@@ -85,6 +85,42 @@ def _rows4(a, name):
     return a
 
 
+def tune_table_dict(t):
+    """A C nb_tune_table as a plain dict."""
+    return {"version": t.version, "sms": t.sms, "device": t.device.decode(),
+            "ap_threads": list(t.ap_threads), "ap_k": list(t.ap_k),
+            "ap_ctas": list(t.ap_ctas), "walk_warps": t.walk_warps,
+            "crossover": [list(r) for r in t.crossover]}
+
+
+def autotune(cache_path=None):
+    """Measures the tuning table on the current device (all-pairs shape per
+    size, walk warps per block, all-pairs / Barnes-Hut crossover per theta
+    class and traversal), installs it and returns it as a dict."""
+    t = L.nb_tune_table()
+    L.check(L.load().nb_autotune(cache_path.encode() if cache_path else None,
+                                 ctypes.byref(t)))
+    return tune_table_dict(t)
+
+
+def tune_get():
+    t = L.nb_tune_table()
+    L.check(L.load().nb_tune_get(ctypes.byref(t)))
+    return tune_table_dict(t)
+
+
+def tune_set(table: dict):
+    """Installs a tuning table (a dict as tune_get returns) by hand."""
+    t = L.nb_tune_table()
+    L.check(L.load().nb_tune_defaults(ctypes.byref(t)))
+    for k in ("ap_threads", "ap_k", "ap_ctas"):
+        getattr(t, k)[:] = table[k]
+    t.walk_warps = table["walk_warps"]
+    for i in range(L.NB_TUNE_THETAS):
+        t.crossover[i][:] = table["crossover"][i]
+    L.check(L.load().nb_tune_set(ctypes.byref(t)))
+
+
 def read_state(path):
     """A state file (checkpoint) or plain ic.bin: dict with pos, vel, lo, acc
     ((n, 4) float32), params (SimParams, None for a plain ic.bin) and flags

@@ -121,19 +121,19 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   return NB_OK;
 }
 
-int ws_reserve_allpairs(Workspace& w, int n, int jsplit) {
+int ws_reserve_allpairs(Workspace& w, int n, const APGeom& g) {
   NB_TRY(ws_basic(w));
   int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
   if (npad > w.src_cap) {
     NB_TRY(dalloc(&w.src, (size_t)npad));   // 2 float4 per pair = npad float4
     w.src_cap = npad;
   }
-  size_t need = jsplit > 1 ? (size_t)jsplit * n : 1;
-  if ((int)need > w.part_cap) {
+  size_t need = g.jsplit > 1 ? (size_t)g.jsplit * n : 1;
+  if (need > (size_t)w.part_cap) {
     NB_TRY(dalloc(&w.part, need));
     w.part_cap = (int)need;
   }
-  int itiles = (n + 1023) / 1024 + 1;
+  int itiles = g.itiles + 1;
   if (itiles > w.tickets_cap) {
     NB_TRY(dalloc(&w.tickets, (size_t)itiles));
     NB_CUDA(cudaMemset(w.tickets, 0, itiles * sizeof(unsigned)));
@@ -239,17 +239,18 @@ static int mark(PhaseMarks* pm, int phase, cudaStream_t st) {
   return NB_OK;
 }
 
-// NB_FORCE_AUTO: all-pairs below the measured crossover, Barnes-Hut above.
-static int resolve_force(int force, int n) {
-  if (force != NB_FORCE_AUTO) return force;
-  return n < NB_AUTO_CROSSOVER ? NB_FORCE_NAIVE : NB_FORCE_BH;
+// NB_FORCE_AUTO: all-pairs below the tuned crossover, Barnes-Hut above.
+static int resolve_force(const nb_params& p, int n) {
+  return resolve_force_tuned(p.force, n, p.theta, p.traverse);
 }
 
 // The whole force evaluation (plus the optional fused kick / drift / kick).
 // n < 2 with Barnes-Hut writes zeros as src/forces_bh.cu:466-469 does.
-static int enqueue_forces(Workspace& w, const StepArgs& a, int force,
-                          cudaStream_t st, PhaseMarks* pm) {
-  force = resolve_force(force, a.n);
+// `force` is NB_FORCE_NAIVE or NB_FORCE_BH (AUTO resolved by the caller).
+int enqueue_forces(Workspace& w, const StepArgs& a, int force, cudaStream_t st,
+                   PhaseMarks* pm) {
+  if (force == NB_FORCE_AUTO)
+    force = resolve_force_tuned(force, a.n, std::sqrt(a.theta2), a.traverse);
   if (pm) NB_CUDA(cudaEventRecord(pm->start, st));
   if (force == NB_FORCE_BH && a.n < 2) {
     if (a.kick_drift) NB_TRY(launch_prep(w, a, false, false, st));
@@ -258,7 +259,7 @@ static int enqueue_forces(Workspace& w, const StepArgs& a, int force,
     return mark(pm, NB_PHASE_WALK, st);
   }
   if (force == NB_FORCE_NAIVE) {
-    NB_TRY(ws_reserve_allpairs(w, a.n, allpairs_geometry(a.n).jsplit));
+    NB_TRY(ws_reserve_allpairs(w, a.n, allpairs_geometry(a.n)));
     NB_TRY(launch_prep(w, a, false, true, st));
     if (a.after_prep) NB_CUDA(cudaEventRecord(a.after_prep, st));
     NB_TRY(mark(pm, NB_PHASE_PREP, st));
@@ -455,10 +456,10 @@ static int sim_capture(nb_sim* s) {
   }
   s->graph_valid = false;
   // reserve first so no allocation happens during capture
-  if (resolve_force(s->p.force, s->n) == NB_FORCE_BH)
+  if (resolve_force(s->p, s->n) == NB_FORCE_BH)
     NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
   else
-    NB_TRY(ws_reserve_allpairs(s->ws, s->n, allpairs_geometry(s->n).jsplit));
+    NB_TRY(ws_reserve_allpairs(s->ws, s->n, allpairs_geometry(s->n)));
   cudaGraph_t g = nullptr;
   NB_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
   int rc = sim_step_eager(s, nullptr);
@@ -554,6 +555,7 @@ int nb_sim_create(int n, const float* pos4, const float* vel4,
   NB_TRY(check_n(n));
   NB_TRY(check_params(p));
   if (!pos4 || !vel4) return set_error(NB_ERR_INVALID, "pos4 / vel4 is NULL");
+  NB_TRY(tune_ensure(nullptr));   // first use on this device: the tuning table
   nb_sim* s = new nb_sim();
   s->n = n;
   s->p = *p;
@@ -866,7 +868,7 @@ int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
 int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts) {
   if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
   int* dcounts = nullptr;
-  if (counts && resolve_force(s->p.force, s->n) == NB_FORCE_BH && s->n >= 2) {
+  if (counts && resolve_force(s->p, s->n) == NB_FORCE_BH && s->n >= 2) {
     NB_TRY(ws_reserve(s->ws, s->n, s->p.key_bits));
     dcounts = s->ws.counts;
   }
@@ -971,7 +973,7 @@ int nb_forces_range_dev(nb_workspace* w, int n, float* d_pos4, float* d_pos_lo4,
     return set_error(NB_ERR_INVALID, "the opening kick needs d_acc4 = a(x)");
   NB_TRY(check_n(n));
   NB_TRY(check_params(p));
-  if (resolve_force(p->force, n) != NB_FORCE_BH)
+  if (resolve_force(*p, n) != NB_FORCE_BH)
     return set_error(NB_ERR_INVALID, "a target range needs Barnes-Hut forces");
   if (t0 < 0 || t1 < t0 || t1 > n || ((t0 & 31) && t0 != n) || ((t1 & 31) && t1 != n))
     return set_error(NB_ERR_INVALID,

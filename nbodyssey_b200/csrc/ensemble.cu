@@ -25,9 +25,12 @@ struct nb_ensemble {
   SimDesc* d_sims = nullptr;
   int* d_blk = nullptr;
   BuildPlan plan;              // tree-build levels (fixed membership)
+  EnsAllPairs ap;              // the all-pairs simulations' work
+  size_t ap_pool_f4 = 0;
   Workspace ews;               // energy scratch
   double* d_energy = nullptr;  // [nsims][6]
   bool primed = false;
+  bool any_tree = false;       // some simulation uses the tree pipeline
   bool use_graphs = true;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t slots[16] = {};
@@ -68,8 +71,8 @@ int ens_check_params(const nb_params& p) {
     return set_error(NB_ERR_INVALID, "theta must be >= 0");
   if (!std::isfinite(p.dt) || !std::isfinite(p.G))
     return set_error(NB_ERR_INVALID, "dt and G must be finite");
-  if (p.force != NB_FORCE_BH)
-    return set_error(NB_ERR_INVALID, "ensembles run the Barnes-Hut module");
+  if (p.force != NB_FORCE_BH && p.force != NB_FORCE_NAIVE && p.force != NB_FORCE_AUTO)
+    return set_error(NB_ERR_INVALID, "force must be NB_FORCE_NAIVE, _BH or _AUTO");
   if (p.traverse != NB_TRAVERSE_THREAD && p.traverse != NB_TRAVERSE_WARP)
     return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
   if (p.key_bits != 30)
@@ -84,10 +87,13 @@ int ens_enqueue(nb_ensemble* h, bool prime) {
   e.kick_after = !prime;
   cudaStream_t st = h->stream;
   NB_TRY(launch_ens_prep(e, st));
-  NB_TRY(launch_ens_morton(e, st));
-  NB_TRY(launch_ens_sort(e, st));
-  NB_TRY(launch_ens_levels(e, h->plan, st));
-  NB_TRY(launch_walk_list_ens(e, st));
+  if (h->any_tree) {
+    NB_TRY(launch_ens_morton(e, st));
+    NB_TRY(launch_ens_sort(e, st));
+    NB_TRY(launch_ens_levels(e, h->plan, st));
+    NB_TRY(launch_walk_list_ens(e, st));
+  }
+  NB_TRY(launch_ens_allpairs(e, h->ap, st));
   return NB_OK;
 }
 
@@ -147,6 +153,7 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     total += n[s];
   }
   if (slots >= (1ll << 29)) return set_error(NB_ERR_INVALID, "too many particles in total");
+  NB_TRY(tune_ensure(nullptr));   // first use on this device: the tuning table
   nb_ensemble* h = new nb_ensemble();
   h->nsims = nsims;
   h->n.assign(n, n + nsims);
@@ -172,8 +179,10 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
       d.theta2 = p.theta * p.theta;
       d.active = 1;
       d.compensated = p.compensated ? 1 : 0;
-      d.pad = 0;
-      coff += n[s];
+      // the module the simulation gets alone (NB_FORCE_AUTO: the tuned
+      // crossover); all-pairs simulations stay out of the tree pipeline
+      d.force = resolve_force_tuned(p.force, n[s], p.theta, p.traverse);
+      if (d.force == NB_FORCE_BH) coff += n[s];
       const int nb32 = (n[s] + 31) / 32;
       for (int k = 0; k < nb32; ++k) blk.push_back(s);
       b += nb32 * 32;
@@ -212,6 +221,16 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     e.status = e.hist + 8 * kSortRadix + 8;
     if ((rc = ens_alloc(h, &e.err, 4)) != NB_OK) break;
     if ((rc = plan_build(sims.data(), nsims, h->plan)) != NB_OK) break;
+    for (const SimDesc& d : sims) h->any_tree |= d.force == NB_FORCE_BH;
+    h->ap_pool_f4 = plan_ens_allpairs(sims.data(), nsims, nullptr, h->ap);
+    if (!h->ap.args.empty()) {
+      EnsAllPairs& ap = h->ap;
+      if ((rc = ens_alloc(h, &ap.d_pool, h->ap_pool_f4)) != NB_OK) break;
+      if ((rc = ens_alloc(h, &ap.d_args, ap.args.size())) != NB_OK) break;
+      if ((rc = ens_alloc(h, &ap.d_items, ap.items.size())) != NB_OK) break;
+      if ((rc = ens_alloc(h, &ap.d_src_off, (size_t)nsims)) != NB_OK) break;
+      if ((rc = ens_alloc(h, &ap.d_counter, 6)) != NB_OK) break;
+    }
     {
       BuildRun* runs = nullptr;
       if ((rc = ens_alloc(h, &runs, h->plan.runs.size())) != NB_OK) break;
@@ -257,7 +276,12 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
                              cudaMemcpyHostToDevice, st);
       row += n[s];
     }
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce == cudaSuccess && h->ap.d_pool)
+      ce = cudaMemsetAsync(h->ap.d_pool, 0, sizeof(float4) * h->ap_pool_f4, st);
+    if (ce != cudaSuccess) { rc = set_error(NB_ERR_CUDA, cudaGetErrorString(ce)); break; }
+    if (!h->ap.args.empty() &&
+        (rc = bind_ens_allpairs(h->ap, sims.data(), nsims, e, st)) != NB_OK) break;
+    ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess) { rc = set_error(NB_ERR_CUDA, cudaGetErrorString(ce)); break; }
   } while (0);
   if (rc != NB_OK) {

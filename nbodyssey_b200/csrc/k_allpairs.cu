@@ -13,6 +13,7 @@
 // * Small n splits the source range over `jsplit` CTAs per target tile; the
 //   last CTA of a tile (ticket) sums the partials in fixed order, so results
 //   are deterministic.  The leapfrog's closing kick is fused in the epilogue.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -56,42 +57,28 @@ constexpr int kStages = 3;
 constexpr int kTileF4 = kSrcTile;                 // float4 per tile (2 per pair)
 constexpr uint32_t kTileBytes = kTileF4 * 16u;   // 8 KB
 
-struct APArgs {
-  int n;
-  const float4* __restrict__ pos;
-  const float4* __restrict__ src;   // packed sources, npad particles
-  int npad;
-  int jsplit;
-  int jchunk;                       // particles per j-chunk (multiple of tile)
-  float eps2, G, half_dt;
-  float4* acc;
-  float4* vel;                      // closing kick or nullptr
-  float4* part;                     // [jsplit][n] partials
-  unsigned* tickets;                // [itiles]
-  unsigned* err;
-};
 
+// One work item: the targets of tile `itile` (THREADS x K of them) against
+// the sources of chunk `jc`, then the tile's fixed-order reduction when this
+// is its last chunk to finish.  `tc` counts the tiles this CTA has taken
+// through its ring so far (stage tc % kStages, barrier phase tc / kStages),
+// so one CTA can run items back to back; every thread of the block calls it.
 template <int THREADS, int K>
-__global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
-  __shared__ __align__(128) float4 s_tile[kStages][kTileF4];
-  __shared__ __align__(8) uint64_t s_bar[kStages];
-  __shared__ bool s_last;
+__device__ __forceinline__ void ap_item(const APArgs& a, int itile, int jc,
+                                        float4 (*s_tile)[kTileF4], uint64_t* s_bar,
+                                        bool* s_last, uint32_t& tc) {
   const int tid = threadIdx.x;
-  const int ibase = blockIdx.x * THREADS * K;
-  const int j0 = blockIdx.y * a.jchunk;
+  const int ibase = itile * THREADS * K;
+  const int j0 = jc * a.jchunk;
   const int j1 = min(j0 + a.jchunk, a.npad);
   const int ntiles = (j1 - j0) / kSrcTile;
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) mbar_init(&s_bar[s], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  }
-  __syncthreads();
-  if (tid == 0) {
-    for (int s = 0; s < kStages && s < ntiles; ++s)
-      bulk_load(s_tile[s], a.src + 2 * ((j0 + s * kSrcTile) / 2), kTileBytes,
-                &s_bar[s]);
+    for (int s = 0; s < kStages && s < ntiles; ++s) {
+      const uint32_t u = tc + s;
+      bulk_load(s_tile[u % kStages], a.src + 2 * ((j0 + s * kSrcTile) / 2), kTileBytes,
+                &s_bar[u % kStages]);
+    }
   }
 
   f2 nx[K], ny[K], nz[K], ax[K], ay[K], az[K];
@@ -112,8 +99,9 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
   // thread and the decision to leave is the whole block's.
   int failed_at = -1;
   for (int t = 0; t < ntiles; ++t) {
-    const int s = t % kStages;
-    const bool landed = mbar_wait(&s_bar[s], (uint32_t)((t / kStages) & 1));
+    const uint32_t u = tc + t;
+    const int s = u % kStages;
+    const bool landed = mbar_wait(&s_bar[s], (u / kStages) & 1u);
     const ulonglong2* tile = reinterpret_cast<const ulonglong2*>(s_tile[s]);
 #pragma unroll 4
     for (int q = 0; q < kSrcTile / 2; ++q) {
@@ -151,10 +139,11 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
   if (!ok && tid == 0) {
     raise_err(a.err, NB_DEVERR_WAIT);
     // let the copies still in flight into this block's shared memory land
-    // (bounded waits) before the block retires
+    // (bounded waits) before the block moves on or retires
     for (int t = failed_at; t < ntiles && t < failed_at + kStages; ++t)
-      mbar_wait(&s_bar[t % kStages], (uint32_t)((t / kStages) & 1));
+      mbar_wait(&s_bar[(tc + t) % kStages], ((tc + t) / kStages) & 1u);
   }
+  tc += ok ? ntiles : min(ntiles, failed_at + kStages);
 
   // A block that could not read its sources writes NaN rows (and, with the
   // j-split, still takes its ticket), so a failed launch leaves visibly
@@ -169,37 +158,41 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
     up2(az[k], u, v); res[k].z = ok ? u + v : bad;
   }
 
+  bool write = true;
   if (a.jsplit > 1) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       int i = ibase + k * THREADS + tid;
       if (i < a.n)
-        a.part[(size_t)blockIdx.y * a.n + i] =
-            make_float4(res[k].x, res[k].y, res[k].z, 0.f);
+        a.part[(size_t)jc * a.n + i] = make_float4(res[k].x, res[k].y, res[k].z, 0.f);
     }
     __threadfence();
     __syncthreads();
     if (tid == 0) {
-      unsigned tk = atomicAdd(&a.tickets[blockIdx.x], 1u);
-      s_last = tk == (unsigned)a.jsplit - 1u;
-      if (s_last) a.tickets[blockIdx.x] = 0u;   // ready for the next launch
+      unsigned tk = atomicAdd(&a.tickets[itile], 1u);
+      *s_last = tk == (unsigned)a.jsplit - 1u;
+      if (*s_last) a.tickets[itile] = 0u;   // ready for the next launch
     }
     __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+    write = *s_last;
+    if (write) {
+      __threadfence();
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      int i = ibase + k * THREADS + tid;
-      float3 sum = make_float3(0.f, 0.f, 0.f);
-      if (i < a.n) {
-        for (int js = 0; js < a.jsplit; ++js) {
-          float4 p = __ldcg(&a.part[(size_t)js * a.n + i]);
-          sum.x += p.x; sum.y += p.y; sum.z += p.z;
+      for (int k = 0; k < K; ++k) {
+        int i = ibase + k * THREADS + tid;
+        float3 sum = make_float3(0.f, 0.f, 0.f);
+        if (i < a.n) {
+          for (int js = 0; js < a.jsplit; ++js) {
+            float4 p = __ldcg(&a.part[(size_t)js * a.n + i]);
+            sum.x += p.x; sum.y += p.y; sum.z += p.z;
+          }
         }
+        res[k] = sum;
       }
-      res[k] = sum;
     }
+    __syncthreads();   // s_last is read by every thread before it is reused
   }
+  if (!write) return;
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     int i = ibase + k * THREADS + tid;
@@ -216,29 +209,93 @@ __global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
   }
 }
 
-// Geometry: 256 threads x 4 targets per CTA; the source range is split so the
-// grid fills the SMs (two CTAs each) several times over.
-APGeom allpairs_geometry(int n) {
+__device__ __forceinline__ void ap_ring_init(uint64_t* s_bar) {
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&s_bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+template <int THREADS, int K>
+__global__ void __launch_bounds__(THREADS) k_allpairs(APArgs a) {
+  __shared__ __align__(128) float4 s_tile[kStages][kTileF4];
+  __shared__ __align__(8) uint64_t s_bar[kStages];
+  __shared__ bool s_last;
+  ap_ring_init(s_bar);
+  uint32_t tc = 0;
+  ap_item<THREADS, K>(a, blockIdx.x, blockIdx.y, s_tile, s_bar, &s_last, tc);
+}
+
+// Many simulations' all-pairs forces in one persistent launch: each CTA pops
+// work items (simulation, target tile, source chunk) from a device queue
+// until it is empty.  Each simulation keeps the source chunking (jsplit) of
+// its own geometry, so its sums, and its results, equal the ones it gets
+// alone.  Items are ordered longest chunks first.
+
+template <int THREADS, int K>
+__global__ void __launch_bounds__(THREADS) k_allpairs_queue(APQueue q) {
+  __shared__ __align__(128) float4 s_tile[kStages][kTileF4];
+  __shared__ __align__(8) uint64_t s_bar[kStages];
+  __shared__ bool s_last;
+  __shared__ int s_item;
+  ap_ring_init(s_bar);
+  uint32_t tc = 0;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();   // read by all before thread 0 writes the next one
+    if (it >= q.nitems) break;
+    const int4 w = q.items[it];
+    APArgs a = q.sims[w.x];
+    if (!q.kick) a.vel = nullptr;
+    ap_item<THREADS, K>(a, w.y, w.z, s_tile, s_bar, &s_last, tc);
+  }
+}
+
+// Geometry: THREADS x K targets per CTA (the compiled shapes below); the
+// source range is split over jsplit CTAs per target tile so that about
+// `ctas` CTAs are in flight (the tuning table's choice for this size).
+APGeom allpairs_geometry_for(int n, int threads, int k, int ctas) {
   APGeom g;
-  g.threads = 256;
-  g.k = 4;
+  g.threads = threads;
+  g.k = k;
   const int per = g.threads * g.k;
   g.itiles = (n + per - 1) / per;
   const int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
   const int jtiles = npad / kSrcTile;
-  const int target = device_sm_count() * 2 * 4;   // CTAs wanted in flight over the launch
-  int js = (target + g.itiles - 1) / g.itiles;
+  int js = (ctas + g.itiles - 1) / g.itiles;
   if (js > jtiles) js = jtiles;
   if (js < 1) js = 1;
   // round the chunk to whole tiles and recompute the split it implies
-  int jt_per = (jtiles + js - 1) / js;
+  const int jt_per = (jtiles + js - 1) / js;
   g.jsplit = (jtiles + jt_per - 1) / jt_per;
   return g;
 }
 
-int launch_allpairs(Workspace& w, const StepArgs& s, cudaStream_t st) {
-  APGeom g = allpairs_geometry(s.n);
-  NB_TRY(ws_reserve_allpairs(w, s.n, g.jsplit));
+APGeom allpairs_geometry(int n) {
+  int threads = 256, k = 4, ctas = 0;
+  tune_allpairs(n, &threads, &k, &ctas);
+  return allpairs_geometry_for(n, threads, k, ctas);
+}
+
+bool allpairs_shape_compiled(int threads, int k) {
+  return (threads == 128 || threads == 256) && (k == 2 || k == 4 || k == 8);
+}
+
+template <int T, int K>
+static void launch_ap(const APArgs& a, const APGeom& g, cudaStream_t st) {
+  k_allpairs<T, K><<<dim3(g.itiles, g.jsplit), T, 0, st>>>(a);
+}
+
+int launch_allpairs_geom(Workspace& w, const StepArgs& s, const APGeom& g,
+                         cudaStream_t st) {
+  if (!allpairs_shape_compiled(g.threads, g.k))
+    return set_error(NB_ERR_INVALID, "all-pairs shape " + std::to_string(g.threads) +
+                                         " x " + std::to_string(g.k) + " is not compiled");
+  NB_TRY(ws_reserve_allpairs(w, s.n, g));
   APArgs a;
   a.n = s.n;
   a.pos = s.pos;
@@ -255,9 +312,171 @@ int launch_allpairs(Workspace& w, const StepArgs& s, cudaStream_t st) {
   a.part = w.part;
   a.tickets = w.tickets;
   a.err = w.err;
-  dim3 grid(g.itiles, g.jsplit);
-  k_allpairs<256, 4><<<grid, 256, 0, st>>>(a);
+  switch (g.threads * 16 + g.k) {
+    case 128 * 16 + 2: launch_ap<128, 2>(a, g, st); break;
+    case 128 * 16 + 4: launch_ap<128, 4>(a, g, st); break;
+    case 128 * 16 + 8: launch_ap<128, 8>(a, g, st); break;
+    case 256 * 16 + 2: launch_ap<256, 2>(a, g, st); break;
+    case 256 * 16 + 8: launch_ap<256, 8>(a, g, st); break;
+    default: launch_ap<256, 4>(a, g, st); break;
+  }
   NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
+int launch_allpairs(Workspace& w, const StepArgs& s, cudaStream_t st) {
+  return launch_allpairs_geom(w, s, allpairs_geometry(s.n), st);
+}
+
+// ---------------------------------------------------------------------------
+// Batches (ensembles, the server): the all-pairs simulations' work.
+// ---------------------------------------------------------------------------
+
+// Packs the sources of the all-pairs simulations: warp b takes 32-slot block
+// b; a simulation's slots past its n are zero-mass pads, as are the packed
+// pairs past its last block (the buffer is zeroed once).
+__global__ void k_ens_pack(EnsArgs e, const int* __restrict__ src_off,
+                           float4* __restrict__ src) {
+  const int lane = threadIdx.x & 31;
+  const int blk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (blk >= e.nblocks) return;
+  const int s = e.blk_sim[blk];
+  if (s < 0) return;
+  const SimDesc d = e.sims[s];
+  const int off = src_off[s];
+  if (off < 0 || !d.active) return;
+  const int local = blk * 32 - d.base + lane;
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (local < d.n) p = e.pos[blk * 32 + lane];
+  const float x1 = __shfl_down_sync(0xffffffffu, p.x, 1);
+  const float y1 = __shfl_down_sync(0xffffffffu, p.y, 1);
+  const float z1 = __shfl_down_sync(0xffffffffu, p.z, 1);
+  const float m1 = __shfl_down_sync(0xffffffffu, p.w, 1);
+  if (!(lane & 1)) {
+    float4* q = src + off + local;   // pair local / 2 at float4 2 (local / 2)
+    q[0] = make_float4(p.x, x1, p.y, y1);
+    q[1] = make_float4(p.z, z1, p.w, m1);
+  }
+}
+
+size_t ap_region_f4(int n) {
+  const APGeom g = allpairs_geometry(n);
+  const size_t npad = (size_t)(n + kSrcTile - 1) / kSrcTile * kSrcTile;
+  const size_t part = g.jsplit > 1 ? (size_t)g.jsplit * n : 0;
+  const size_t tick = ((size_t)g.itiles + 3) / 4;
+  return (npad + part + tick + 15) / 16 * 16;
+}
+
+size_t plan_ens_allpairs(const SimDesc* sims, int nsims, const size_t* region_of,
+                         EnsAllPairs& ap) {
+  ap.args.clear();
+  ap.sim.clear();
+  ap.region.clear();
+  ap.items.clear();
+  ap.groups.clear();
+  ap.src_off.assign(nsims, -1);
+  struct Pending { int a; APGeom g; };
+  std::vector<Pending> todo;
+  size_t next = 0, top = 0;
+  for (int s = 0; s < nsims; ++s) {
+    const SimDesc& d = sims[s];
+    if (!d.active || d.force != NB_FORCE_NAIVE) continue;
+    const APGeom g = allpairs_geometry(d.n);
+    const int npad = (d.n + kSrcTile - 1) / kSrcTile * kSrcTile;
+    APArgs a{};
+    a.n = d.n;
+    a.npad = npad;
+    a.jsplit = g.jsplit;
+    a.jchunk = (npad / kSrcTile + g.jsplit - 1) / g.jsplit * kSrcTile;
+    a.eps2 = d.eps2;
+    a.G = d.G;
+    a.half_dt = d.half_dt;
+    const size_t r = region_of ? region_of[s] : next;
+    next = r + ap_region_f4(d.n);
+    top = std::max(top, next);
+    ap.src_off[s] = (int)r;
+    todo.push_back({(int)ap.args.size(), g});
+    ap.args.push_back(a);
+    ap.sim.push_back(s);
+    ap.region.push_back(r);
+  }
+  // one group per launch shape; items longest chunks first
+  for (int threads : {128, 256})
+    for (int k : {2, 4, 8}) {
+      EnsAllPairs::Group grp{threads, k, (int)ap.items.size(), 0};
+      std::vector<int4> its;
+      for (const Pending& p : todo) {
+        if (p.g.threads != threads || p.g.k != k) continue;
+        for (int jc = 0; jc < p.g.jsplit; ++jc)
+          for (int it = 0; it < p.g.itiles; ++it) its.push_back(make_int4(p.a, it, jc, 0));
+      }
+      if (its.empty()) continue;
+      std::stable_sort(its.begin(), its.end(), [&](const int4& x, const int4& y) {
+        return ap.args[x.x].jchunk > ap.args[y.x].jchunk;
+      });
+      ap.items.insert(ap.items.end(), its.begin(), its.end());
+      grp.nitems = (int)its.size();
+      ap.groups.push_back(grp);
+    }
+  return top;
+}
+
+int bind_ens_allpairs(EnsAllPairs& ap, const SimDesc* sims, int nsims, const EnsArgs& e,
+                      cudaStream_t st) {
+  for (size_t i = 0; i < ap.args.size(); ++i) {
+    const SimDesc& d = sims[ap.sim[i]];
+    APArgs& a = ap.args[i];
+    float4* reg = ap.d_pool + ap.region[i];
+    a.pos = e.pos + d.base;
+    a.src = reg;
+    a.acc = e.acc + d.base;
+    a.vel = (d.active == 1) ? e.vel + d.base : nullptr;
+    a.part = reg + a.npad;
+    a.tickets = reinterpret_cast<unsigned*>(reg + a.npad + (a.jsplit > 1 ? (size_t)a.jsplit * a.n : 0));
+    a.err = e.err;
+  }
+  if (!ap.args.empty())
+    NB_CUDA(cudaMemcpyAsync(ap.d_args, ap.args.data(), sizeof(APArgs) * ap.args.size(),
+                            cudaMemcpyHostToDevice, st));
+  if (!ap.items.empty())
+    NB_CUDA(cudaMemcpyAsync(ap.d_items, ap.items.data(), sizeof(int4) * ap.items.size(),
+                            cudaMemcpyHostToDevice, st));
+  NB_CUDA(cudaMemcpyAsync(ap.d_src_off, ap.src_off.data(), sizeof(int) * nsims,
+                          cudaMemcpyHostToDevice, st));
+  return NB_OK;
+}
+
+template <int T, int K>
+static void launch_queue(const APQueue& q, int grid, cudaStream_t st) {
+  k_allpairs_queue<T, K><<<grid, T, 0, st>>>(q);
+}
+
+int launch_ens_allpairs(const EnsArgs& e, const EnsAllPairs& ap, cudaStream_t st) {
+  if (ap.groups.empty()) return NB_OK;
+  k_ens_pack<<<(e.nblocks * 32 + 255) / 256, 256, 0, st>>>(e, ap.d_src_off, ap.d_pool);
+  NB_CUDA(cudaGetLastError());
+  NB_CUDA(cudaMemsetAsync(ap.d_counter, 0, sizeof(int) * ap.groups.size(), st));
+  const int sms = device_sm_count();
+  for (size_t gi = 0; gi < ap.groups.size(); ++gi) {
+    const EnsAllPairs::Group& g = ap.groups[gi];
+    APQueue q;
+    q.sims = ap.d_args;
+    q.items = ap.d_items + g.first_item;
+    q.nitems = g.nitems;
+    q.counter = ap.d_counter + gi;
+    q.kick = e.kick_after ? 1 : 0;
+    // persistent: about two CTAs of 256 threads per SM, no more than items
+    const int grid = std::min(g.nitems, sms * (g.threads == 128 ? 4 : 2));
+    switch (g.threads * 16 + g.k) {
+      case 128 * 16 + 2: launch_queue<128, 2>(q, grid, st); break;
+      case 128 * 16 + 4: launch_queue<128, 4>(q, grid, st); break;
+      case 128 * 16 + 8: launch_queue<128, 8>(q, grid, st); break;
+      case 256 * 16 + 2: launch_queue<256, 2>(q, grid, st); break;
+      case 256 * 16 + 8: launch_queue<256, 8>(q, grid, st); break;
+      default: launch_queue<256, 4>(q, grid, st); break;
+    }
+    NB_CUDA(cudaGetLastError());
+  }
   return NB_OK;
 }
 
@@ -465,7 +684,8 @@ extern "C" int nb_compute_forces_naive_static(int n, const float* d_pos4,
   unsigned* tail = (unsigned*)(base + kStaticSrcBytes + kStaticPartBytes);
   NB_CUDA(cudaMemsetAsync(tail, 0, kStaticTailBytes, st));
 
-  APGeom g = allpairs_geometry(n);
+  // a fixed shape (256 x 4, 8 CTAs per SM wanted), independent of tuning
+  APGeom g = allpairs_geometry_for(n, 256, 4, device_sm_count() * 8);
   const int npad = (n + kSrcTile - 1) / kSrcTile * kSrcTile;
   const int jtiles = npad / kSrcTile;
   int js = g.jsplit < kStaticMaxSplit ? g.jsplit : kStaticMaxSplit;

@@ -1046,7 +1046,7 @@ __global__ void __launch_bounds__(256) k_ens_morton(EnsArgs e) {
     if (s >= 0) {
       const SimDesc d = e.sims[s];
       const int local = slot - d.base;
-      if (d.active && local < d.n) {
+      if (d.active && d.force == NB_FORCE_BH && local < d.n) {
         const float lx = ord2f(e.bbox_min[4 * s]), ly = ord2f(e.bbox_min[4 * s + 1]),
                     lz = ord2f(e.bbox_min[4 * s + 2]);
         const float hx = ord2f(e.bbox_max[4 * s]), hy = ord2f(e.bbox_max[4 * s + 1]),
@@ -1125,7 +1125,7 @@ int plan_build(const SimDesc* sims, int nsims, BuildPlan& plan) {
   std::vector<int> groups(nsims, 0), first(nsims, 0);
   int live = 0;
   for (int s = 0; s < nsims; ++s)
-    if (sims[s].active && sims[s].n >= 2) {
+    if (sims[s].active && sims[s].n >= 2 && sims[s].force == NB_FORCE_BH) {
       groups[s] = (sims[s].n + kLeafGroup - 1) / kLeafGroup;
       ++live;
     }

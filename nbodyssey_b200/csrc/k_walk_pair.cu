@@ -39,21 +39,21 @@
 
 namespace nb {
 
-constexpr int kPW = 4;            // warps per block
 constexpr int kPStack = 512;      // opened-node entries per warp
 constexpr int kPRing = 128;       // interaction-list ring entries per warp
 constexpr int kPFlush = 32;       // entries evaluated per flush
 constexpr int kPAmb = 64;         // children staged for the all-target test
 
-template <bool MASKED>
+// Shared memory of a block of W warps.
+template <int W, bool MASKED>
 struct PairSmem {
-  int stk[kPW][kPStack];
-  unsigned smask[kPW][MASKED ? kPStack : 1];
-  __align__(16) float ent[kPW][kPRing * 4];
-  unsigned emask[kPW][MASKED ? kPRing : 1];
-  __align__(16) float amb[kPW][kPAmb * 4];
-  unsigned res[kPW][kPAmb];
-  float4 ext[kPW][MASKED ? 1 : 6];
+  int stk[W][kPStack];
+  unsigned smask[W][MASKED ? kPStack : 1];
+  __align__(16) float ent[W][kPRing * 4];
+  unsigned emask[W][MASKED ? kPRing : 1];
+  __align__(16) float amb[W][kPAmb * 4];
+  unsigned res[W][kPAmb];
+  float4 ext[W][MASKED ? 1 : 6];
 };
 
 __device__ __forceinline__ float pw_min(float v) {
@@ -106,9 +106,9 @@ __device__ __forceinline__ float box_far2(float cx, float cy, float cz, float lo
 }
 
 // The walk of warp `wg` (targets 32wg .. 32wg+31); all 32 lanes call it.
-template <bool MASKED, bool COUNT, bool HOIST = false>
+template <int W, bool MASKED, bool COUNT, bool HOIST = false>
 __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
-                                               PairSmem<MASKED>& sm) {
+                                               PairSmem<W, MASKED>& sm) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int n = a.n, ni = n - 1;
@@ -389,25 +389,28 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
   }
 }
 
-template <bool MASKED, bool COUNT>
-__global__ void __launch_bounds__(kPW * 32) k_walk_pair(WalkArgs a) {
-  __shared__ PairSmem<MASKED> sm;
-  walk_pair_warp<MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * kPW + (threadIdx.x >> 5), sm);
+template <int W, bool MASKED, bool COUNT>
+__global__ void __launch_bounds__(W * 32) k_walk_pair(WalkArgs a) {
+  __shared__ PairSmem<W, MASKED> sm;
+  walk_pair_warp<W, MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
 }
 
 // Ensemble: each warp takes one 32-slot block of the concatenated sorted
 // arrays; blocks belong to one simulation (bases are multiples of 32), whose
 // tree, parameters and semantics the walk uses.  Simulations with the other
 // semantics are left to the other instantiation.
+constexpr int kEnsW = 4;
 template <bool MASKED>
-__global__ void __launch_bounds__(kPW * 32) k_walk_pair_ens(EnsArgs e) {
-  __shared__ PairSmem<MASKED> sm;
-  const int blk = blockIdx.x * kPW + (threadIdx.x >> 5);
+__global__ void __launch_bounds__(kEnsW * 32) k_walk_pair_ens(EnsArgs e) {
+  __shared__ PairSmem<kEnsW, MASKED> sm;
+  const int blk = blockIdx.x * kEnsW + (threadIdx.x >> 5);
   if (blk >= e.nblocks) return;
   const int s = e.blk_sim[blk];
   if (s < 0) return;
   const SimDesc d = e.sims[s];
-  if (!d.active || d.n < 2 || (d.traverse == NB_TRAVERSE_THREAD) != MASKED) return;
+  if (!d.active || d.n < 2 || d.force != NB_FORCE_BH ||
+      (d.traverse == NB_TRAVERSE_THREAD) != MASKED)
+    return;
   WalkArgs a;
   a.n = d.n;
   a.ps = e.pos_sorted + d.base;
@@ -426,29 +429,42 @@ __global__ void __launch_bounds__(kPW * 32) k_walk_pair_ens(EnsArgs e) {
   a.t0 = 0;
   a.t1 = d.n;
   a.part = nullptr;
-  walk_pair_warp<MASKED, false, true>(a, blk - d.base / 32, sm);
+  walk_pair_warp<kEnsW, MASKED, false, true>(a, blk - d.base / 32, sm);
 }
 
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
-  const int blocks = (e.nblocks + kPW - 1) / kPW;
+  const int blocks = (e.nblocks + kEnsW - 1) / kEnsW;
   if (blocks == 0) return NB_OK;
-  k_walk_pair_ens<false><<<blocks, kPW * 32, 0, st>>>(e);
-  k_walk_pair_ens<true><<<blocks, kPW * 32, 0, st>>>(e);
+  k_walk_pair_ens<false><<<blocks, kEnsW * 32, 0, st>>>(e);
+  k_walk_pair_ens<true><<<blocks, kEnsW * 32, 0, st>>>(e);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }
 
+template <int W>
+static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaStream_t st) {
+  if (masked) {
+    // the lane masks double the stack: thread semantics stay at <= 4 warps
+    // per block (<= 32 KB of static shared memory)
+    constexpr int WM = W < 4 ? W : 4;
+    const int bm = (blocks * W + WM - 1) / WM;
+    if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
+    else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
+  } else {
+    if (a.counts) k_walk_pair<W, false, true><<<blocks, W * 32, 0, st>>>(a);
+    else k_walk_pair<W, false, false><<<blocks, W * 32, 0, st>>>(a);
+  }
+}
+
+// The block shape (warps per block) is the tuning table's.
 int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
   const int warps = (a.t1 - a.t0 + 31) / 32;
   if (warps <= 0) return NB_OK;
-  const int blocks = (warps + kPW - 1) / kPW;
-  if (masked) {
-    if (a.counts) k_walk_pair<true, true><<<blocks, kPW * 32, 0, st>>>(a);
-    else k_walk_pair<true, false><<<blocks, kPW * 32, 0, st>>>(a);
-  } else {
-    if (a.counts) k_walk_pair<false, true><<<blocks, kPW * 32, 0, st>>>(a);
-    else k_walk_pair<false, false><<<blocks, kPW * 32, 0, st>>>(a);
-  }
+  const int W = tune_walk_warps();
+  const int blocks = (warps + W - 1) / W;
+  if (W == 2) launch_walk_pair_w<2>(a, masked, blocks, st);
+  else if (W == 8) launch_walk_pair_w<8>(a, masked, blocks, st);
+  else launch_walk_pair_w<4>(a, masked, blocks, st);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }

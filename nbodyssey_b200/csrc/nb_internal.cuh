@@ -138,7 +138,8 @@ constexpr int kPrepThreads = 256;
 constexpr int kPrepMaxBlocks = 1024;
 
 int ws_reserve(Workspace& w, int n, int key_bits);
-int ws_reserve_allpairs(Workspace& w, int n, int jsplit);
+struct APGeom;
+int ws_reserve_allpairs(Workspace& w, int n, const APGeom& g);
 int ws_reserve_energy(Workspace& w, int n, int blocks, int jsplit);
 void ws_free(Workspace& w);
 
@@ -190,14 +191,65 @@ int launch_flush(void* buf, size_t bytes, cudaStream_t st);
 int device_sm_count();
 int measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
 
-// all-pairs launch geometry (autotuned by n)
+// Arguments of the all-pairs kernel (one simulation).
+struct APArgs {
+  int n;
+  const float4* __restrict__ pos;
+  const float4* __restrict__ src;   // packed sources, npad particles
+  int npad;
+  int jsplit;
+  int jchunk;                       // particles per j-chunk (multiple of tile)
+  float eps2, G, half_dt;
+  float4* acc;
+  float4* vel;                      // closing kick or nullptr
+  float4* part;                     // [jsplit][n] partials
+  unsigned* tickets;                // [itiles]
+  unsigned* err;
+};
+
+// The persistent all-pairs launch over many simulations' work items.
+struct APQueue {
+  const APArgs* sims;     // per-simulation arguments (pointers into its slots)
+  const int4* items;      // (simulation, target tile, source chunk, -)
+  int nitems;
+  int* counter;           // next item; zeroed before the launch
+  int kick;               // closing kick of the simulations that step
+};
+
+// all-pairs launch geometry
 struct APGeom {
   int threads;   // per CTA
   int k;         // targets per thread
   int jsplit;    // CTAs along j per i-tile
   int itiles;
 };
+// the tuning table's geometry for n particles on the current device
 APGeom allpairs_geometry(int n);
+// a given shape with about `ctas` CTAs in flight
+APGeom allpairs_geometry_for(int n, int threads, int k, int ctas);
+bool allpairs_shape_compiled(int threads, int k);
+int launch_allpairs_geom(Workspace& w, const StepArgs& a, const APGeom& g,
+                         cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Tuning table (tune.cu): per device, measured on it at first use or loaded
+// from its cache file.
+// ---------------------------------------------------------------------------
+// all-pairs shape and CTAs in flight for n particles
+void tune_allpairs(int n, int* threads, int* k, int* ctas);
+// Barnes-Hut walk: warps per block
+int tune_walk_warps();
+// NB_FORCE_AUTO: all-pairs below this many particles, Barnes-Hut from there
+int tune_crossover(float theta, int traverse);
+// resolves NB_FORCE_AUTO for n particles (other methods pass through)
+int resolve_force_tuned(int force, int n, float theta, int traverse);
+// first use on the current device: load the cache file or measure the table
+// (never while `st` is capturing); idempotent
+int tune_ensure(cudaStream_t st);
+// the whole force evaluation of one step (api.cu)
+struct PhaseMarks;
+int enqueue_forces(Workspace& w, const StepArgs& a, int force, cudaStream_t st,
+                   PhaseMarks* pm);
 
 // ---------------------------------------------------------------------------
 // Ensembles: many simulations in one set of arrays.  Simulation s owns slots
@@ -215,7 +267,7 @@ struct SimDesc {
   float half_dt, dt, eps2, G, theta2;
   int active;     // 0: skipped; 1: stepped; 2: a(x) only (newly admitted)
   int compensated;
-  int pad;
+  int force;      // NB_FORCE_BH (tree pipeline) or NB_FORCE_NAIVE (all-pairs)
 };
 
 constexpr int kEnsSimBits = 10;                     // sim id field of the keys
@@ -275,6 +327,45 @@ struct EnsArgs {
   int2* seg[2];               // open splits between build levels
   int* seg_count[2];
 };
+
+// All-pairs work of the simulations of a batch that use the all-pairs
+// module (k_allpairs.cu): each has a region of a float4 pool holding its
+// packed sources, its partials and its tile tickets, its own launch geometry
+// (the one it gets alone, so its sums and results are the same), and the
+// queue items of one persistent launch per launch shape.
+struct EnsAllPairs {
+  struct Group {
+    int threads, k, first_item, nitems;
+  };
+  std::vector<APArgs> args;    // per all-pairs simulation
+  std::vector<int> sim;        // its index in the simulation table
+  std::vector<size_t> region;  // its region offset in the pool (float4)
+  std::vector<int4> items;     // (all-pairs simulation, target tile, chunk, -)
+  std::vector<Group> groups;
+  std::vector<int> src_off;    // per simulation: pool offset of its packed
+                               // sources, -1 for one without all-pairs work
+  // device (owned by the batch)
+  float4* d_pool = nullptr;
+  APArgs* d_args = nullptr;
+  int4* d_items = nullptr;
+  int* d_src_off = nullptr;    // [nsims]
+  int* d_counter = nullptr;    // [6] one per launch shape
+};
+// Pool float4 of one simulation's region (sources, partials, tickets); its
+// sources come first and must start zeroed, its tickets too.
+size_t ap_region_f4(int n);
+// Host plan of the simulations whose SimDesc.force is NB_FORCE_NAIVE and that
+// are active: geometry, items, and the region of simulation s at
+// region_of[s] (nullptr: back to back from 0).  Returns the pool size used.
+size_t plan_ens_allpairs(const SimDesc* sims, int nsims, const size_t* region_of,
+                         EnsAllPairs& ap);
+// Points the per-simulation arguments at the batch's arrays and the pool and
+// uploads them with the items and source offsets (stream-ordered; the host
+// vectors must live until the copies ran).
+int bind_ens_allpairs(EnsAllPairs& ap, const SimDesc* sims, int nsims, const EnsArgs& e,
+                      cudaStream_t st);
+// Packs the all-pairs simulations' sources, then the queue launches.
+int launch_ens_allpairs(const EnsArgs& e, const EnsAllPairs& ap, cudaStream_t st);
 
 int launch_ens_prep(const EnsArgs& e, cudaStream_t st);
 int launch_ens_morton(const EnsArgs& e, cudaStream_t st);

@@ -41,6 +41,8 @@ constexpr size_t kBytesPerSlot = 272;   // state 64, sorted 16, keys 16, perm 8,
                                         // sort scratch ~12, build plan and
                                         // segments ~4
 constexpr int kInFlight = 2;            // engine steps queued ahead of the GPU
+constexpr int kApChunk = 1024;          // all-pairs scratch allocation unit (float4)
+constexpr int kApPoolShare = 8;         // 1 / 8 of the budget: all-pairs scratch
 constexpr int kFrameSlots = 8;
 
 double now_s() {
@@ -59,6 +61,9 @@ struct Request {
   int state = 0;              // 0 queued, 1 running, 2 done, 3 failed
   int sim = -1;
   int base = -1;
+  int force = NB_FORCE_BH;    // the module it gets alone (AUTO resolved)
+  int ap_chunk = -1;          // all-pairs: its region in the scratch pool
+  int ap_len = 0;             // (units of kApChunk float4)
   int steps_done = 0;
   int frames = 0;
   bool primed = false;
@@ -87,6 +92,15 @@ struct nb_server {
   std::vector<SimDesc> sims;         // host mirror, by sim id
   std::vector<int> blk;              // host mirror of blk_sim
   std::map<int, int> free_blocks;    // start block -> length (32-slot blocks)
+  // all-pairs requests: packed sources, partials and tickets per request in
+  // regions of a scratch pool, and the persistent launch's work items
+  float4* d_ap_pool = nullptr;
+  int ap_chunks = 0;
+  std::map<int, int> ap_free;        // start chunk -> length
+  std::vector<size_t> ap_region;     // by sim id: region offset (float4)
+  EnsAllPairs ap;
+  size_t ap_items_cap = 0;
+  bool any_tree = false;
   std::vector<int> free_ids;
   bool table_dirty = false;
   BuildPlan plan;                    // tree-build levels of the running sims
@@ -138,34 +152,36 @@ int srv_alloc(nb_server* s, T** p, size_t count) {
   return NB_OK;
 }
 
-// first fit over 32-slot blocks; returns the first block or -1
-int take_blocks(nb_server* s, int nblk) {
-  for (auto it = s->free_blocks.begin(); it != s->free_blocks.end(); ++it) {
-    if (it->second >= nblk) {
-      int start = it->first, len = it->second;
-      s->free_blocks.erase(it);
-      if (len > nblk) s->free_blocks[start + nblk] = len - nblk;
+// first fit over a free list (start -> length); returns the start or -1
+int take_range(std::map<int, int>& fl, int len) {
+  for (auto it = fl.begin(); it != fl.end(); ++it) {
+    if (it->second >= len) {
+      int start = it->first, have = it->second;
+      fl.erase(it);
+      if (have > len) fl[start + len] = have - len;
       return start;
     }
   }
   return -1;
 }
 
-void give_blocks(nb_server* s, int start, int nblk) {
-  auto it = s->free_blocks.emplace(start, nblk).first;
+void give_range(std::map<int, int>& fl, int start, int len) {
+  auto it = fl.emplace(start, len).first;
   auto nx = std::next(it);
-  if (nx != s->free_blocks.end() && start + it->second == nx->first) {
+  if (nx != fl.end() && start + it->second == nx->first) {
     it->second += nx->second;
-    s->free_blocks.erase(nx);
+    fl.erase(nx);
   }
-  if (it != s->free_blocks.begin()) {
+  if (it != fl.begin()) {
     auto pv = std::prev(it);
     if (pv->first + pv->second == it->first) {
       pv->second += it->second;
-      s->free_blocks.erase(it);
+      fl.erase(it);
     }
   }
 }
+
+int ap_chunks_of(int n) { return (int)((ap_region_f4(n) + kApChunk - 1) / kApChunk); }
 
 int mkdirs(const std::string& path) {
   std::string cur;
@@ -232,7 +248,11 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
     r->done_ev = nullptr;
     const int nb32 = (r->n + 31) / 32;
     for (int b = 0; b < nb32; ++b) s->blk[r->base / 32 + b] = -1;
-    give_blocks(s, r->base / 32, nb32);
+    give_range(s->free_blocks, r->base / 32, nb32);
+    if (r->ap_chunk >= 0) {
+      give_range(s->ap_free, r->ap_chunk, r->ap_len);
+      r->ap_chunk = -1;
+    }
     s->free_ids.push_back(r->sim);
     s->table_dirty = true;
     r->state = 2;
@@ -246,8 +266,24 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
     Request* r = s->waiting[k];
     const int nb32 = (r->n + 31) / 32;
     if (s->free_ids.empty()) break;
-    const int b0 = take_blocks(s, nb32);
-    if (b0 < 0) { ++k; continue; }
+    int ap0 = -1;
+    if (r->force == NB_FORCE_NAIVE) {
+      ap0 = take_range(s->ap_free, ap_chunks_of(r->n));
+      if (ap0 < 0) { ++k; continue; }
+    }
+    const int b0 = take_range(s->free_blocks, nb32);
+    if (b0 < 0) {
+      if (ap0 >= 0) give_range(s->ap_free, ap0, ap_chunks_of(r->n));
+      ++k;
+      continue;
+    }
+    if (ap0 >= 0) {
+      r->ap_chunk = ap0;
+      r->ap_len = ap_chunks_of(r->n);
+      // sources start with zero-mass pads and tickets at zero
+      NB_CUDA(cudaMemsetAsync(s->d_ap_pool + (size_t)ap0 * kApChunk, 0,
+                              sizeof(float4) * kApChunk * (size_t)r->ap_len, s->stream));
+    }
     std::sort(s->free_ids.begin(), s->free_ids.end(), std::greater<int>());
     const int id = s->free_ids.back();
     s->free_ids.pop_back();
@@ -272,6 +308,8 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
     d.theta2 = r->p.theta * r->p.theta;
     d.active = 2;   // a(x0) in the step it joins
     d.compensated = r->p.compensated ? 1 : 0;
+    d.force = r->force;
+    s->ap_region[id] = r->ap_chunk >= 0 ? (size_t)r->ap_chunk * kApChunk : 0;
     for (int b = 0; b < nb32; ++b) s->blk[b0 + b] = id;
     s->table_dirty = true;
     s->running.push_back(r);
@@ -290,10 +328,12 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
       extent = std::max(extent, s->sims[id].base + (s->sims[id].n + 31) / 32 * 32);
   if (s->table_dirty) {
     int coff = 0;
+    s->any_tree = false;
     for (int id = 0; id < nsims; ++id)
-      if (s->sims[id].active) {
+      if (s->sims[id].active && s->sims[id].force == NB_FORCE_BH) {
         s->sims[id].coff = coff;
         coff += s->sims[id].n;
+        s->any_tree = true;
       }
     // pageable sources: the calls return once the data is staged, so the
     // host mirrors may change right after; the device copies stay in stream
@@ -309,6 +349,16 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
       NB_CUDA(cudaMemcpyAsync((void*)s->e.runs, s->plan.runs.data(),
                               sizeof(BuildRun) * s->plan.runs.size(),
                               cudaMemcpyHostToDevice, s->stream));
+    plan_ens_allpairs(s->sims.data(), nsims, s->ap_region.data(), s->ap);
+    if (s->ap.items.size() > s->ap_items_cap) {   // grow-only, rare
+      NB_CUDA(cudaStreamSynchronize(s->stream));
+      if (s->ap.d_items) cudaFree(s->ap.d_items);
+      s->ap.d_items = nullptr;
+      const size_t cap = std::max(s->ap.items.size() * 2, (size_t)4096);
+      NB_CUDA(cudaMalloc(&s->ap.d_items, sizeof(int4) * cap));
+      s->ap_items_cap = cap;
+    }
+    NB_TRY(bind_ens_allpairs(s->ap, s->sims.data(), nsims, s->e, s->stream));
     s->table_dirty = false;
   }
   // bound the queue depth: wait for the step issued kInFlight iterations ago
@@ -327,10 +377,13 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
   e.kick_drift = true;
   e.kick_after = true;
   NB_TRY(launch_ens_prep(e, s->stream));
-  NB_TRY(launch_ens_morton(e, s->stream));
-  NB_TRY(launch_ens_sort(e, s->stream));
-  NB_TRY(launch_ens_levels(e, s->plan, s->stream));
-  NB_TRY(launch_walk_list_ens(e, s->stream));
+  if (s->any_tree) {
+    NB_TRY(launch_ens_morton(e, s->stream));
+    NB_TRY(launch_ens_sort(e, s->stream));
+    NB_TRY(launch_ens_levels(e, s->plan, s->stream));
+    NB_TRY(launch_walk_list_ens(e, s->stream));
+  }
+  NB_TRY(launch_ens_allpairs(e, s->ap, s->stream));
   NB_CUDA(cudaEventRecord(ev, s->stream));
   s->step_count += 1;
   if (s->busy_first == 0) s->busy_first = now_s();
@@ -411,16 +464,26 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
   *out = nullptr;
   if (max_sims <= 0 || max_sims > kEnsMaxSims)
     return set_error(NB_ERR_INVALID, "max_sims must be in [1, 1023]");
-  size_t slots = hbm_budget_bytes / kBytesPerSlot / 4096 * 4096;
+  // the slot pool takes all but 1 / kApPoolShare of the budget; the rest is
+  // the all-pairs requests' scratch
+  const size_t ap_bytes = hbm_budget_bytes / kApPoolShare;
+  size_t slots = (hbm_budget_bytes - ap_bytes) / kBytesPerSlot / 4096 * 4096;
   if (slots < 4096) return set_error(NB_ERR_INVALID, "HBM budget too small");
   if (slots > ((size_t)1 << 28)) slots = (size_t)1 << 28;
+  NB_TRY(tune_ensure(nullptr));   // first use on this device: the tuning table
   nb_server* s = new nb_server();
   s->budget = hbm_budget_bytes;
   s->cap_slots = (int)slots;
   s->max_sims = max_sims;
+  s->ap_chunks = (int)std::min<size_t>(ap_bytes / (16 * kApChunk), (size_t)1 << 30);
   int rc = NB_OK;
   do {
     EnsArgs& e = s->e;
+    if ((rc = srv_alloc(s, &s->d_ap_pool, (size_t)s->ap_chunks * kApChunk)) != NB_OK) break;
+    s->ap.d_pool = s->d_ap_pool;
+    if ((rc = srv_alloc(s, &s->ap.d_args, (size_t)max_sims)) != NB_OK) break;
+    if ((rc = srv_alloc(s, &s->ap.d_src_off, (size_t)max_sims)) != NB_OK) break;
+    if ((rc = srv_alloc(s, &s->ap.d_counter, 6)) != NB_OK) break;
     const size_t S = slots;
     SimDesc* dsims = nullptr;
     int* dblk = nullptr;
@@ -498,8 +561,10 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     return set_error(rc, keep);
   }
   s->sims.assign(max_sims, SimDesc{});
+  s->ap_region.assign(max_sims, 0);
   s->blk.assign(s->cap_slots / 32, -1);
   s->free_blocks[0] = s->cap_slots / 32;
+  if (s->ap_chunks > 0) s->ap_free[0] = s->ap_chunks;
   for (int id = max_sims - 1; id >= 0; --id) s->free_ids.push_back(id);
   s->t_start = now_s();
   int dev = 0;
@@ -538,6 +603,7 @@ int nb_server_destroy(nb_server* s) {
     cudaEventDestroy(s->frame_copied[k]);
   }
   for (void* p : s->dallocs) cudaFree(p);
+  if (s->ap.d_items) cudaFree(s->ap.d_items);
   if (s->h_frame) cudaFreeHost(s->h_frame);
   cudaStreamDestroy(s->stream);
   cudaStreamDestroy(s->side);
@@ -554,11 +620,17 @@ int nb_server_submit(nb_server* s, int n, const float* pos4, const float* vel4,
   if (!(p->eps > 0.f) || !std::isfinite(p->eps) || !(p->theta >= 0.f) ||
       !std::isfinite(p->dt) || !std::isfinite(p->G))
     return set_error(NB_ERR_INVALID, "eps > 0, theta >= 0, finite dt and G required");
-  if (p->force != NB_FORCE_BH || p->key_bits != 30 ||
+  if ((p->force != NB_FORCE_BH && p->force != NB_FORCE_NAIVE && p->force != NB_FORCE_AUTO) ||
+      p->key_bits != 30 ||
       (p->traverse != NB_TRAVERSE_THREAD && p->traverse != NB_TRAVERSE_WARP))
-    return set_error(NB_ERR_INVALID, "the server runs Barnes-Hut with 30-bit keys");
+    return set_error(NB_ERR_INVALID, "the server runs all-pairs, Barnes-Hut or AUTO "
+                                     "with 30-bit keys");
   if ((size_t)(n + 31) / 32 * 32 > (size_t)s->cap_slots)
     return set_error(NB_ERR_NOMEM, "request larger than the server's HBM budget");
+  const int force = resolve_force_tuned(p->force, n, p->theta, p->traverse);
+  if (force == NB_FORCE_NAIVE && ap_chunks_of(n) > s->ap_chunks)
+    return set_error(NB_ERR_NOMEM, "all-pairs request larger than the server's "
+                                   "all-pairs scratch (1/8 of the HBM budget)");
   if (dump_every > 0 && n > s->frame_cap)
     return set_error(NB_ERR_INVALID, "frames of more than 2^21 particles are not streamed");
   if (out_dir && *out_dir && mkdirs(out_dir) != NB_OK)
@@ -566,6 +638,7 @@ int nb_server_submit(nb_server* s, int n, const float* pos4, const float* vel4,
   std::unique_ptr<Request> r(new Request());
   r->n = n;
   r->p = *p;
+  r->force = force;
   r->steps = steps;
   r->dump_every = dump_every;
   r->out_dir = out_dir ? out_dir : "";

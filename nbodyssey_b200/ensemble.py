@@ -20,7 +20,8 @@ from .api import SimParams
 class Ensemble:
     def __init__(self, states, params):
         """states: list of (pos4, vel4) float32 (n, 4) arrays; params: one
-        SimParams (Barnes-Hut) for all, or a list with one per simulation."""
+        SimParams for all, or a list with one per simulation (Barnes-Hut,
+        all-pairs or AUTO, which picks by the tuned crossover)."""
         self._lib = L.load()
         if isinstance(params, SimParams):
             params = [params] * len(states)

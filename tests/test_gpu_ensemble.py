@@ -11,7 +11,7 @@ from nbodyssey_b200.ensemble import Ensemble
 pytestmark = pytest.mark.gpu
 
 
-def _mix():
+def _mix(forces=("bh",)):
     sizes = [1, 2, 33, 1000, 4097, 20_000, 64, 3000]
     states, params = [], []
     for k, n in enumerate(sizes):
@@ -23,14 +23,17 @@ def _mix():
             states[-1] = (p, np.zeros_like(p))
         else:
             states[-1] = (states[-1][0][:n], states[-1][1][:n])
-        params.append(api.SimParams(dt=0.005, epsilon=0.05, force="bh",
+        params.append(api.SimParams(dt=0.005, epsilon=0.05, force=forces[k % len(forces)],
                                     theta=(0.3, 0.5, 0.7)[k % 3],
                                     traverse=("warp", "thread")[k % 2]))
     return states, params
 
 
-def test_ensemble_equals_alone():
-    states, params = _mix()
+@pytest.mark.parametrize("forces", [("bh",), ("naive", "auto", "bh"), ("naive",)])
+def test_ensemble_equals_alone(forces):
+    """Barnes-Hut, all-pairs (the persistent work-queue launch) and
+    NB_FORCE_AUTO simulations side by side: each equals itself alone."""
+    states, params = _mix(forces)
     steps = 4
     with Ensemble(states, params) as ens:
         ens.step(steps)
@@ -50,7 +53,7 @@ def test_ensemble_equals_alone():
 
 
 def test_ensemble_graph_and_eager_identical():
-    states, params = _mix()
+    states, params = _mix(("naive", "bh"))
     out = []
     for graphs in (True, False):
         with Ensemble(states, params) as ens:
@@ -64,7 +67,7 @@ def test_ensemble_graph_and_eager_identical():
 def test_ensemble_rejects_unsupported_params():
     pos, vel = ic.two_disks(100, seed=1)
     with pytest.raises(L.NbError) as ei:
-        Ensemble([(pos, vel)], api.SimParams(force="naive"))
+        Ensemble([(pos, vel)], api.SimParams(force="bh", key_bits=63))
     assert ei.value.code == L.NB_ERR_INVALID
     with pytest.raises(L.NbError):
-        Ensemble([(pos, vel)], api.SimParams(force="bh", key_bits=63))
+        Ensemble([(pos, vel)], api.SimParams(force="bh", epsilon=0.0))

@@ -98,13 +98,29 @@ def test_theta0_equals_allpairs(traverse, walk):
 
 
 def test_compare_forces_gate():
-    """gpu_bench.sh's gate on --compare-forces at theta 0 (mean < 1e-4)."""
-    pos, vel = ic.two_disks(20_000, seed=14)
+    """gpu_bench.sh's gate on --compare-forces at theta 0 (mean < 1e-4), at the
+    N = 100,000 of the 1M workload's exactness gate."""
+    pos, vel = ic.two_disks(100_000, seed=14)
     for tv in ("thread", "warp"):
         prm = api.SimParams(epsilon=EPS, theta=0.0, force="bh", traverse=tv)
         with api.Simulation(pos, vel, prm) as sim:
             mx, mean = sim.compare_forces()
         assert mean < 1e-4 and mx < 1e-3
+
+
+@pytest.mark.parametrize("traverse", ["thread", "warp"])
+def test_theta0_100k_equals_fp64_allpairs(traverse):
+    """The theta = 0 exactness gate at N = 100,000: every target touches all
+    n leaves, and the forces of a seeded 2,048-target subsample are within
+    the FP32 all-pairs band of the FP64 exact force."""
+    n = 100_000
+    pos, _ = ic.two_disks(n, seed=15)
+    acc, cnt = bh_forces(pos, 0.0, traverse)
+    assert (cnt == n).all()
+    tg = np.random.default_rng(15).choice(n, 2048, replace=False)
+    r = rel_err(acc[tg], O.allpairs_f64(pos, EPS, targets=tg))
+    assert r.mean() < 1e-4
+    assert np.median(r) < 1e-5 and np.percentile(r, 99) < 1e-3
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 33, 511, 512, 513, 4096, 12_000, 50_001])

@@ -17,7 +17,7 @@ from nbodyssey_b200.server import DONE, Server
 pytestmark = pytest.mark.gpu
 
 
-def _request(k):
+def _request(k, forces=("bh",)):
     n = (3000, 40, 17_000, 2, 9000, 1)[k % 6]
     if n == 1:
         p = np.array([[0.25, 0.5, -0.5, 0.3]], np.float32)
@@ -25,7 +25,7 @@ def _request(k):
     else:
         pos, vel = ic.two_disks(max(n, 2), seed=200 + k, impact=2.0 + k % 5)
         pos, vel = pos[:n], vel[:n]
-    prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh",
+    prm = api.SimParams(dt=0.005, epsilon=0.05, force=forces[k % len(forces)],
                         theta=(0.3, 0.5, 0.7)[k % 3],
                         traverse=("warp", "thread")[k % 2])
     steps = (7, 3, 12, 5, 9, 4)[k % 6]
@@ -68,6 +68,28 @@ def test_results_identical_alone_and_in_the_mix(tmp_path):
     assert formats.read_frame(str(tmp_path / "f0" / names[0])).shape == reqs[0][0].shape
 
 
+def test_all_pairs_and_auto_requests_identical_alone():
+    """All-pairs requests (the persistent work-queue launch, scratch from the
+    all-pairs pool), AUTO and Barnes-Hut requests in one stream: each result
+    equals the request run alone."""
+    reqs = [_request(k, ("naive", "auto", "bh", "naive")) for k in range(12)]
+    with Server(hbm_budget_bytes=256 << 20, max_sims=6) as srv:
+        ids = []
+        for k, (pos, vel, prm, steps) in enumerate(reqs):
+            ids.append(srv.submit(pos, vel, prm, steps))
+            if k % 3 == 2:
+                time.sleep(0.01)
+        for rid in ids:
+            srv.wait(rid, 120)
+        results = [srv.result(rid) for rid in ids]
+        st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    for (pos, vel, prm, steps), (p, v) in zip(reqs, results):
+        ap, av = _alone(pos, vel, prm, steps)
+        assert np.array_equal(p, ap)
+        assert np.array_equal(v, av)
+
+
 def test_concurrent_submitters():
     reqs = [_request(k) for k in range(8)]
     out = {}
@@ -95,8 +117,13 @@ def test_refuses_what_cannot_fit_and_bad_params():
         assert ei.value.code == L.NB_ERR_NOMEM
         small, _ = ic.two_disks(100, seed=3)
         with pytest.raises(L.NbError) as ei:
-            srv.submit(small, small, api.SimParams(force="naive"), 1)
+            srv.submit(small, small, api.SimParams(force="bh", key_bits=63), 1)
         assert ei.value.code == L.NB_ERR_INVALID
+        # an all-pairs request whose scratch exceeds the all-pairs pool
+        mid, _ = ic.two_disks(30_000, seed=4)
+        with pytest.raises(L.NbError) as ei:
+            srv.submit(mid, mid, api.SimParams(force="naive"), 1)
+        assert ei.value.code == L.NB_ERR_NOMEM
         with pytest.raises(L.NbError) as ei:
             srv.result(12345)
         assert ei.value.code == L.NB_ERR_NOTFOUND
