@@ -87,6 +87,9 @@ def parse_args():
                     help="ensemble: batched encounters vs the plain path one at a "
                          "time; serve: request stream through the server vs FIFO")
     ap.add_argument("--nsims", type=int, default=512)
+    ap.add_argument("--ens-force", choices=["auto", "bh", "naive"], default="auto")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served / batched sub-measurements of the default line")
     ap.add_argument("--requests", type=int, default=200)
     ap.add_argument("--serve-nmax", type=int, default=262144)
     ap.add_argument("--serve-smax", type=int, default=500)
@@ -478,7 +481,32 @@ def run_b200(args, rank, world, local, pg):
         line.pop("interactions_per_particle")
     if world == 1 and not args.no_cpu_baseline and args.force == "bh":
         line["cpu_baseline"] = cpu_baseline(args)
+    if world == 1 and not args.no_served and args.force == "bh":
+        line["served"] = served_summary(args)
     print(json.dumps(line), flush=True)
+
+
+def served_summary(args):
+    """The second half of the headline metric at a size that fits beside the
+    1M line: a 48-request served stream and a 128-encounter batched ensemble,
+    each against the same work run one at a time through the plain drop-in
+    path with the same parameters (force auto in both arms)."""
+    srv = serve_measure(48, 131072, 300, 24.0, args.traverse, args.walk, seed=7, smin=50)
+    ens = ensemble_measure(128, 100, 3, 0.5, args.traverse, args.walk, seed=3)
+    return {"metric": "served particle-steps/s + p99 vs plain, equal accuracy",
+            "value": srv["value"], "unit": "particle-steps/s",
+            "config": {"workload": srv["workload"]},
+            "plain_fifo_particle_steps_per_s": srv["plain_fifo_particle_steps_per_s"],
+            "ratio_vs_plain": srv["ratio_vs_plain"],
+            "latency_s": srv["latency_s"], "accuracy": srv["accuracy"],
+            "ensemble": {"workload": "128 encounters, N log-uniform [2048, 131072], "
+                                     "100 steps, force auto (%d all-pairs, crossover %d), "
+                                     "theta 0.5" % (ens["allpairs_sims"], ens["crossover"]),
+                         "value": ens["value"], "unit": "particle-steps/s",
+                         "plain_fifo_particle_steps_per_s":
+                             ens["plain_fifo_particle_steps_per_s"],
+                         "ratio_vs_plain_device": ens["ratio_vs_plain_device"],
+                         "wall_s": ens["wall_s"]}}
 
 
 def run_shard(args, rank, world, local, pg):
@@ -573,25 +601,22 @@ def run_shard(args, rank, world, local, pg):
     print(json.dumps(line), flush=True)
 
 
-def run_ensemble(args, rank, world, local, pg):
-    """Batched encounters: nsims simulations (N log-uniform in [2048, 131072],
-    mass ratio U[0.25,1], impact U[2,8], inclination U[0,90] deg, approach
-    U[0.3,0.7]; BH theta 0.5 warp walk, eps 0.05, dt 0.005), all advanced
-    together, against the same simulations run one at a time through the
-    plain handle path (create, steps, download, destroy).  Ranks shard the
-    simulations with no collective."""
-    from nbodyssey_b200 import _lib as L
+def ensemble_measure(nsims, steps, warmup, theta, traverse, walk, seed=0,
+                     rank=0, world=1, pg=None, force="auto"):
+    """Batched encounters against the same simulations one at a time through
+    the plain handle path (create, steps, download, destroy), both with the
+    same parameters (force "auto": all-pairs or Barnes-Hut per simulation by
+    the tuned crossover, so both arms have the same method and accuracy per
+    simulation).  Ranks shard the simulations with no collective."""
     from nbodyssey_b200 import api, ic
     from nbodyssey_b200.ensemble import Ensemble, shard
-    lib = L.load()
-    L.check(lib.nb_set_device(local))
-    specs = ic.ensemble_specs(args.nsims, seed=0)
+    specs = ic.ensemble_specs(nsims, seed=seed)
     mine = shard([s["n"] for s in specs], rank, world)
     states = [ic.from_spec(specs[i]) for i in mine]
-    prm = api.SimParams(dt=0.005, epsilon=0.05, theta=args.theta, force="bh",
-                        traverse=args.traverse, walk_kernel=args.walk)
+    prm = api.SimParams(dt=0.005, epsilon=0.05, theta=theta, force=force,
+                        traverse=traverse, walk_kernel=walk)
     parts = sum(p.shape[0] for p, _ in states)
-    K, W = args.steps, args.warmup
+    K, W = steps, warmup
 
     # batched: device time of K steps (graph), and wall time end to end
     dist_barrier(pg)
@@ -614,6 +639,7 @@ def run_ensemble(args, rank, world, local, pg):
     dist_barrier(pg)
     t0 = time.perf_counter()
     plain_ms = 0.0
+    n_allpairs = 0
     for pos, vel in states:
         sim = api.Simulation(pos, vel, prm)
         sim.step(W)
@@ -628,48 +654,69 @@ def run_ensemble(args, rank, world, local, pg):
     wall_p = time.perf_counter() - t0
     plain_ms = dist_max(pg, plain_ms)
     wall_p = dist_max(pg, wall_p)
-    total_parts = sum(s["n"] for s in specs)   # all ranks' shares together
+    tune = api.tune_get()
+    x = tune["crossover"][1][1 if traverse == "warp" else 0]
+    n_allpairs = sum(1 for sp in specs if force == "naive" or (force == "auto" and sp["n"] < x))
+    total_parts = sum(sp["n"] for sp in specs)   # all ranks' shares together
     assert world > 1 or parts == total_parts
-    if rank != 0:
-        return
     value = total_parts * K / (dev_ms * 1e-3)
     plain = total_parts * K / (plain_ms * 1e-3)
-    line = {"metric": "particle-steps/s, batched ensemble of %d encounters" % args.nsims,
-            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": K,
-            "warmup": W, "ms_per_step": dev_ms / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: seeded encounter recipe",
-            "config": {"workload": "ensemble of %d BH theta %.2g %s encounters, N "
-                                   "log-uniform [2048, 131072]" % (args.nsims, args.theta,
-                                                                  args.traverse),
-                       "particles": total_parts, "l2": "inputs larger than L2"},
+    return {"value": value, "unit": "particle-steps/s", "steps": K, "warmup": W,
+            "ms_per_step": dev_ms / K, "particles": total_parts, "nsims": nsims,
             "plain_fifo_particle_steps_per_s": plain,
             "ratio_vs_plain_device": value / plain,
             "wall_s": {"batched": wall_b, "plain_fifo": wall_p,
                        "ratio": wall_p / wall_b},
-            "gpu_launches": ENS_KERNELS_PER_STEP * K}
+            "force": force, "allpairs_sims": n_allpairs,
+            "crossover": x}
+
+
+def run_ensemble(args, rank, world, local, pg):
+    """The batched ensemble workload alone (--workload ensemble)."""
+    from nbodyssey_b200 import _lib as L
+    lib = L.load()
+    L.check(lib.nb_set_device(local))
+    r = ensemble_measure(args.nsims, args.steps, args.warmup, args.theta, args.traverse,
+                         args.walk, rank=rank, world=world, pg=pg, force=args.ens_force)
+    if rank != 0:
+        return
+    line = {"metric": "particle-steps/s, batched ensemble of %d encounters" % args.nsims,
+            "value": r["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": r["steps"], "warmup": r["warmup"], "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic: seeded encounter recipe",
+            "config": {"workload": "ensemble of %d %s theta %.2g %s encounters, N "
+                                   "log-uniform [2048, 131072]" % (args.nsims, args.ens_force,
+                                                                  args.theta, args.traverse),
+                       "particles": r["particles"], "l2": "inputs larger than L2"},
+            "plain_fifo_particle_steps_per_s": r["plain_fifo_particle_steps_per_s"],
+            "ratio_vs_plain_device": r["ratio_vs_plain_device"],
+            "wall_s": r["wall_s"], "allpairs_sims": r["allpairs_sims"],
+            "crossover": r["crossover"],
+            "gpu_launches": ENS_KERNELS_PER_STEP * r["steps"]}
     print(json.dumps(line), flush=True)
 
 
-def serve_requests(args, rng):
-    """The request stream: N log-uniform in [4096, nmax], steps U[100, smax],
+def serve_requests(requests, nmax, smax, traverse, walk, rng, smin=100):
+    """The request stream: N log-uniform in [4096, nmax], steps U[smin, smax],
     theta from {0.3, 0.5, 0.7}, encounter geometry as the ensemble recipe, a
-    frame every 50 steps."""
+    frame every 50 steps; force "auto" (all-pairs or Barnes-Hut per request
+    by the tuned crossover, the same for the served and the plain arm)."""
     from nbodyssey_b200 import api, ic
     import math
     reqs = []
-    for k in range(args.requests):
-        n = int(round(math.exp(rng.uniform(math.log(4096), math.log(args.serve_nmax)))))
+    for k in range(requests):
+        n = int(round(math.exp(rng.uniform(math.log(4096), math.log(nmax)))))
         spec = dict(n=n, mass_ratio=float(rng.uniform(0.25, 1.0)),
                     impact=float(rng.uniform(2.0, 8.0)),
                     inclination_deg=float(rng.uniform(0.0, 90.0)),
                     approach=float(rng.uniform(0.3, 0.7)),
                     seed=int(rng.integers(0, 2 ** 31 - 1)))
         pos, vel = ic.from_spec(spec)
-        prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh",
+        prm = api.SimParams(dt=0.005, epsilon=0.05, force="auto",
                             theta=float(rng.choice([0.3, 0.5, 0.7])),
-                            traverse=args.traverse, walk_kernel=args.walk)
-        steps = int(rng.integers(100, args.serve_smax + 1))
+                            traverse=traverse, walk_kernel=walk)
+        steps = int(rng.integers(smin, smax + 1))
         reqs.append((pos, vel, prm, steps))
     return reqs
 
@@ -680,21 +727,17 @@ def _pcts(lat):
             "p99": float(np.percentile(lat, 99))}
 
 
-def run_serve(args, rank, world, local, pg):
+def serve_measure(requests, nmax, smax, budget_gb, traverse, walk, seed, smin=100):
     """Served request stream vs FIFO one at a time through the plain path.
     (1) capacity: every request submitted at t=0, particle-steps/s;
     (2) latency: Poisson arrivals at 80 % of the plain path's capacity, the
     same arrival times for both, p50/p95/p99 completion latency."""
-    import threading
-    from nbodyssey_b200 import _lib as L
     from nbodyssey_b200 import api
     from nbodyssey_b200.server import Server
-    lib = L.load()
-    L.check(lib.nb_set_device(local))
-    rng = np.random.default_rng(1000 + rank)
-    reqs = serve_requests(args, rng)
+    rng = np.random.default_rng(seed)
+    reqs = serve_requests(requests, nmax, smax, traverse, walk, rng, smin=smin)
     work = float(sum(p.shape[0] * s for p, _, _, s in reqs))
-    budget = int(args.hbm_budget_gb * (1 << 30))
+    budget = int(budget_gb * (1 << 30))
 
     def plain_one(pos, vel, prm, steps):
         with api.Simulation(pos, vel, prm) as sim:
@@ -737,7 +780,7 @@ def run_serve(args, rank, world, local, pg):
             lat[k] = time.perf_counter() - (t0 + ta)
         return time.perf_counter() - t0, lat
 
-    plain_one(*reqs[0])                      # warm-up (JIT-free, but pages in)
+    plain_one(*reqs[0])                      # warm-up (pages in the library)
     zero = [0.0] * len(reqs)
     wall_s, _, st = serve_all(zero)
     wall_f, _ = fifo_all(zero)
@@ -747,18 +790,15 @@ def run_serve(args, rank, world, local, pg):
     arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs))).tolist()
     _, lat_s, st2 = serve_all(arrivals)
     _, lat_f = fifo_all(arrivals)
-    if rank != 0:
-        return
-    line = {"metric": "served particle-steps/s + p99 vs plain (request stream)",
-            "value": cap_s, "unit": "particle-steps/s", "n_gpus": world,
-            "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic request stream",
-            "config": {"workload": "%d requests, N log-uniform [4096, %d], steps "
-                                   "U[100, %d], theta {0.3,0.5,0.7}, frame every 50 "
-                                   "steps, HBM budget %.0f GB" %
-                                   (args.requests, args.serve_nmax, args.serve_smax,
-                                    args.hbm_budget_gb),
-                       "particle_steps": work},
+    tune = api.tune_get()
+    n_ap = sum(1 for p, _, prm, _ in reqs
+               if p.shape[0] < tune["crossover"][[0.3, 0.5, 0.7].index(round(prm.theta, 1))]
+               [1 if traverse == "warp" else 0])
+    return {"value": cap_s, "unit": "particle-steps/s",
+            "workload": "%d requests, N log-uniform [4096, %d], steps U[%d, %d], theta "
+                        "{0.3,0.5,0.7}, force auto (%d all-pairs), frame every 50 steps, "
+                        "HBM budget %.0f GB" % (requests, nmax, smin, smax, n_ap, budget_gb),
+            "particle_steps": work,
             "plain_fifo_particle_steps_per_s": cap_f,
             "ratio_vs_plain": cap_s / cap_f,
             "latency_s": {"served": _pcts(lat_s), "plain_fifo": _pcts(lat_f),
@@ -766,7 +806,27 @@ def run_serve(args, rank, world, local, pg):
                           "load": "80 % of the plain path's capacity"},
             "server": {"peak_running": st["peak_running"],
                        "engine_steps": st["engine_steps"], "frames": st["frames"],
-                       "frame_bytes": st["frame_bytes"]}}
+                       "frame_bytes": st["frame_bytes"]},
+            "accuracy": "equal: each request's result is bit-identical served and "
+                        "alone (tests/test_gpu_server.py)"}
+
+
+def run_serve(args, rank, world, local, pg):
+    """The served request stream alone (--workload serve)."""
+    from nbodyssey_b200 import _lib as L
+    lib = L.load()
+    L.check(lib.nb_set_device(local))
+    r = serve_measure(args.requests, args.serve_nmax, args.serve_smax, args.hbm_budget_gb,
+                      args.traverse, args.walk, seed=1000 + rank)
+    if rank != 0:
+        return
+    line = {"metric": "served particle-steps/s + p99 vs plain (request stream)",
+            "value": r["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic request stream",
+            "config": {"workload": r["workload"], "particle_steps": r["particle_steps"]}}
+    line.update({k: r[k] for k in ("plain_fifo_particle_steps_per_s", "ratio_vs_plain",
+                                    "latency_s", "server", "accuracy")})
     print(json.dumps(line), flush=True)
 
 
