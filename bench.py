@@ -305,10 +305,14 @@ def measured_peaks():
         return {}
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the walk kernel from the committed ncu
-    summary (profiles/), if present."""
-    path = os.path.join(ROOT, "profiles", "walk_list_1m.md")
+def profiled_traffic(kernel):
+    """Per-launch DRAM bytes of the timed force kernel from its committed ncu
+    summary (profiles/<kernel>_1m.md, the same 1M workload), if present."""
+    name = {"k_walk_pair": "walk_pair_1m.md", "k_walk_list": "walk_list_1m.md",
+            "k_walk_warp": "walk_warp_dfs_1m.md"}.get(kernel)
+    if name is None:
+        return None
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -431,7 +435,9 @@ def run_b200(args, rank, world, local, pg):
     build_ms = sum(phases[k] for k in ("prep", "morton", "sort", "build", "com")) / calls
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
-    traffic = profiled_traffic()
+    kernel = ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
+        args.walk, "k_walk_%s" % args.traverse) if args.force == "bh" else "k_allpairs")
+    traffic = profiled_traffic(kernel) if args.n == N_DEFAULT else None
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -455,9 +461,7 @@ def run_b200(args, rank, world, local, pg):
                 "path": "nb_step_host: pinned host pos / vel / a(x) in, one step, "
                         "pos / vel / a(x_new) out (positions return on a second "
                         "stream during the tree build and walk), wall clock"},
-        "roofline": {"kernel": ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
-                                    args.walk, "k_walk_%s" % args.traverse) if args.force == "bh"
-                                else "k_allpairs"), "bound": "fp32",
+        "roofline": {"kernel": kernel, "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": traffic,
                      "work": ("20 flop x per-thread-criterion interactions "

@@ -230,6 +230,15 @@ NB_API int nb_flush_l2(nb_sim* s, size_t bytes);
 NB_API int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
                   int32_t* children, int32_t* parent, float* com4,
                   float* size2);
+/* Debug / parity: the child-pair records of the tree built on the current
+ * positions (the layout the tree walk reads), n - 1 records of 12 floats:
+ * record k = (x_l, x_r, y_l, y_r, z_l, z_r, m_l, m_r, size2_l, size2_r,
+ * w_l, w_r) for the two children of the internal node that splits after
+ * sorted leaf k (left: node or leaf k, right: node or leaf k + 1); an
+ * internal child gives its centre of mass, mass, squared box edge and split
+ * (w, the bits of an int32), a leaf its position, mass, size2 = -1 and
+ * w = -1. */
+NB_API int nb_debug_pairs(nb_sim* s, float* rec12);
 /* Debug / parity: forces with per-particle interaction counts (original
  * order; warp mode counts the warp's shared walk for every lane). */
 NB_API int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts);

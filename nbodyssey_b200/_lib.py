@@ -127,6 +127,7 @@ SIGNATURES = {
     "nb_set_graphs": (_I, [_P, _I]),
     "nb_debug_lbvh": (_I, [_P, _P, _P, _P, _P, _P, _P]),
     "nb_debug_forces": (_I, [_P, _P, _P]),
+    "nb_debug_pairs": (_I, [_P, _P]),
     "nb_compare_forces": (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
     "nb_workspace_create": (_I, [_PP]),
     "nb_workspace_destroy": (_I, [_P]),

@@ -341,6 +341,13 @@ class Simulation:
             L.ptr(out["parent"]), L.ptr(out["com4"]), L.ptr(out["size2"])))
         return out
 
+    def debug_pairs(self):
+        """The tree's child-pair records, (n - 1, 12) float32 (see
+        nb_debug_pairs in include/nbody_b200.h)."""
+        out = np.empty((self.n - 1, 12), np.float32)
+        L.check(self._lib.nb_debug_pairs(self._h, L.ptr(out)))
+        return out
+
     def debug_forces(self):
         """(acc4, interaction counts), original order."""
         acc = np.empty((self.n, 4), np.float32)

@@ -865,6 +865,17 @@ int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
   return rc;
 }
 
+int nb_debug_pairs(nb_sim* s, float* rec12) {
+  if (!s || !rec12) return set_error(NB_ERR_INVALID, "NULL argument");
+  if (s->n < 2) return set_error(NB_ERR_INVALID, "n must be >= 2 for a tree");
+  // the records of the tree last built on the current positions
+  NB_TRY(nb_debug_lbvh(s, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr));
+  NB_CUDA(cudaMemcpyAsync(rec12, s->ws.pairs, sizeof(PairRec) * (size_t)(s->n - 1),
+                          cudaMemcpyDeviceToHost, s->stream));
+  NB_CUDA(cudaStreamSynchronize(s->stream));
+  return check_device_error(s->ws, s->stream);
+}
+
 int nb_debug_forces(nb_sim* s, float* acc4, int32_t* counts) {
   if (!s) return set_error(NB_ERR_INVALID, "sim is NULL");
   int* dcounts = nullptr;

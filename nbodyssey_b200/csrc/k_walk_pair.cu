@@ -151,8 +151,9 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
   int head = 0;   // ring position of the first unevaluated entry (multiple of 32)
   int lc = 0;     // unevaluated entries
 
-  // list pair q of the 32-entry block at ring position `at`
-  auto pair_term = [&](int at, int q) {
+  // list pair q of the 32-entry block at ring position `at`; (qx, qy, qz)
+  // the packed negated target and e2 the packed eps^2, made once per block
+  auto pair_term = [&](int at, int q, f2 qx, f2 qy, f2 qz, f2 e2) {
     const float* base = &ent[at * 4];
     const ulonglong2 A = *reinterpret_cast<const ulonglong2*>(&base[q * 8]);
     const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&base[q * 8 + 4]);
@@ -165,10 +166,10 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
       if (COUNT) cnt += (int)(b0 + b1);
     }
-    f2 dx = add2(A.x, px());
-    f2 dy = add2(A.y, py());
-    f2 dz = add2(B.x, pz());
-    f2 r2 = fma2(dz, dz, HOIST ? he2 : pk2u(a.eps2));
+    f2 dx = add2(A.x, qx);
+    f2 dy = add2(A.y, qy);
+    f2 dz = add2(B.x, qz);
+    f2 r2 = fma2(dz, dz, e2);
     r2 = fma2(dy, dy, r2);
     r2 = fma2(dx, dx, r2);
     float r0, r1;
@@ -183,8 +184,9 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
   };
   // evaluates the 32 entries at `head` (unrolled, fixed offsets)
   auto flush_full = [&]() {
+    const f2 qx = px(), qy = py(), qz = pz(), e2 = HOIST ? he2 : pk2u(a.eps2);
 #pragma unroll
-    for (int q = 0; q < kPFlush / 2; ++q) pair_term(head, q);
+    for (int q = 0; q < kPFlush / 2; ++q) pair_term(head, q, qx, qy, qz, e2);
     if (!MASKED && COUNT) cnt += kPFlush;
     head = (head + kPFlush) & (kPRing - 1);
     lc -= kPFlush;
@@ -294,10 +296,11 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       }
       __syncwarp();
       const f2 th2 = pk2(theta2, theta2);
+      const f2 qx = px(), qy = py(), qz = pz();
       for (int q = 0; q < (na + 1) >> 1; ++q) {
         const ulonglong2 U = *reinterpret_cast<const ulonglong2*>(&am[q * 8]);
         const ulonglong2 V = *reinterpret_cast<const ulonglong2*>(&am[q * 8 + 4]);
-        const f2 dx = add2(U.x, px()), dy = add2(U.y, py()), dz = add2(V.x, pz());
+        const f2 dx = add2(U.x, qx), dy = add2(U.y, qy), dz = add2(V.x, qz);
         const f2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
         float t0, t1, z0, z1;
         up2(mul2(th2, d2), t0, t1);
@@ -366,7 +369,8 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
         __syncwarp();
       }
       const int np = (lc + 1) >> 1;
-      for (int q = 0; q < np; ++q) pair_term(head, q);
+      const f2 qx = px(), qy = py(), qz = pz(), e2 = HOIST ? he2 : pk2u(a.eps2);
+      for (int q = 0; q < np; ++q) pair_term(head, q, qx, qy, qz, e2);
       if (!MASKED && COUNT) cnt += lc;
     }
     float u, v;

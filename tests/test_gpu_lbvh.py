@@ -95,3 +95,44 @@ def test_large_tree_bit_exact_1m():
     assert np.all(np.diff(t["keys"].astype(np.int64)) >= 0)
     assert np.array_equal(np.sort(t["perm"]), np.arange(1_000_000, dtype=np.uint32))
     assert abs(float(t["com4"][0, 3]) - float(pos[:, 3].astype(np.float64).sum())) < 1e-5
+
+
+def expected_pairs(o):
+    """The child-pair records implied by the oracle's tree: record k holds the
+    children of the internal node whose split is after sorted leaf k."""
+    n = o.n
+    ni = n - 1
+    rec = np.zeros((ni, 12), np.float32)
+    for p in range(ni):
+        l, r = int(o.children[p, 0]), int(o.children[p, 1])
+        k = l if l < ni else l - ni   # the node's split: its left child's index
+        for side, c in ((0, l), (1, r)):
+            if c >= ni:   # leaf
+                x, y, z, m = o.pos_sorted[c - ni]
+                s2, w = np.float32(-1.0), -1
+            else:
+                x, y, z, m = o.com[c]
+                s2 = o.size2[c]
+                cl = int(o.children[c, 0])
+                w = cl if cl < ni else cl - ni
+            rec[k, side] = x
+            rec[k, 2 + side] = y
+            rec[k, 4 + side] = z
+            rec[k, 6 + side] = m
+            rec[k, 8 + side] = s2
+            rec[k, 10 + side] = np.int32(w).view(np.float32)
+    return rec
+
+
+@pytest.mark.parametrize("n", [2, 3, 33, 1025, 4097, 20_001])
+@pytest.mark.parametrize("bits", [30, 63])
+def test_child_pair_records_bit_exact(n, bits):
+    """Every child-pair record the build writes (the walk's input) equals the
+    record derived from the oracle's tree, bits of the floats included."""
+    pos, _ = ic.two_disks(max(n, 4), seed=n + 7)
+    pos = pos[:n]
+    prm = api.SimParams(epsilon=0.05, theta=0.5, force="bh", traverse="warp", key_bits=bits)
+    with api.Simulation(pos, np.zeros_like(pos), prm) as sim:
+        rec = sim.debug_pairs()
+    exp = expected_pairs(O.Tree(pos, bits))
+    assert np.array_equal(rec.view(np.int32), exp.view(np.int32))
