@@ -99,3 +99,22 @@ def test_energy_band_12k_bh_2000_steps(traverse):
             worst = max(worst, abs(sim.energy()[0] - e0) / abs(e0))
     print("12k BH theta 0.5 %s, 2000 steps: max |dE/E| = %.3g" % (traverse, worst))
     assert worst <= 5e-3
+
+
+def test_energy_gate_12k_bh_accuracy_setting():
+    """The opening angle at which Barnes-Hut meets the 2e-4 energy gate on
+    the 12,000-particle workload over 2,000 steps.  The monopole drift
+    follows the force error, not the step: measured with the oracle's walk
+    (the same interaction sets, FP64 sums) at theta 0.5 / 0.4 / 0.3 / 0.2 /
+    0.15 / 0.1: 3.2e-3 / 2.5e-3 / 1.4e-3 / 6.0e-4 / 3.1e-4 / 1.0e-4, and
+    3.2e-3 at theta 0.5 with half the step over the same time."""
+    pos, vel = ic.two_disks(12_000, seed=0)
+    prm = api.SimParams(dt=0.005, epsilon=0.05, force="bh", theta=0.1, traverse="warp")
+    with api.Simulation(pos, vel, prm) as sim:
+        e0 = sim.energy()[0]
+        worst = 0.0
+        for _ in range(20):
+            sim.step(100)
+            worst = max(worst, abs(sim.energy()[0] - e0) / abs(e0))
+    print("12k BH theta 0.1, 2000 steps: max |dE/E| = %.3g" % worst)
+    assert worst <= 2e-4
