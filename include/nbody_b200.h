@@ -42,7 +42,7 @@ extern "C" {
 #define NB_DEVERR_STACK 1u  /* a tree walk's stack would have overflowed */
 #define NB_DEVERR_SORT 2u   /* a radix-sort look-back wait hit its limit */
 #define NB_DEVERR_WAIT 4u   /* a bulk-copy barrier wait hit its limit */
-#define NB_DEVERR_QUEUE 8u  /* a persistent work-queue wait hit its limit */
+#define NB_DEVERR_QUEUE 8u  /* a persistent work-queue item was out of range (skipped) */
 #define NB_DEVERR_TREE 16u  /* the centre-of-mass climb met an inconsistent tree */
 #define NB_DEVERR_VISITS 32u /* a tree walk visited more nodes than the tree has */
 #define NB_DEVERR_BOUNDS 64u /* a tree-build write outside its tree (skipped) */

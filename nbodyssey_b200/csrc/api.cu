@@ -300,7 +300,7 @@ static int check_device_error(Workspace& w, cudaStream_t st) {
     if (e & NB_DEVERR_BOUNDS) m += " (tree-build write out of range, skipped)";
     if (e & NB_DEVERR_SORT) m += " (radix sort look-back wait limit)";
     if (e & NB_DEVERR_WAIT) m += " (bulk-copy barrier wait limit)";
-    if (e & NB_DEVERR_QUEUE) m += " (work-queue wait limit)";
+    if (e & NB_DEVERR_QUEUE) m += " (work-queue item out of range, skipped)";
     return set_error(NB_ERR_DEVICE, m);
   }
   return NB_OK;

@@ -248,8 +248,16 @@ __global__ void __launch_bounds__(THREADS) k_allpairs_queue(APQueue q) {
     const int it = s_item;
     __syncthreads();   // read by all before thread 0 writes the next one
     if (it >= q.nitems) break;
-    const int4 w = q.items[it];
+    const int4 w = q.items[it];   // the same item for every thread: uniform
+    if (w.x < 0 || w.x >= q.nsims) {
+      if (threadIdx.x == 0) raise_err(q.err, NB_DEVERR_QUEUE);
+      continue;
+    }
     APArgs a = q.sims[w.x];
+    if (w.y < 0 || (long long)w.y * THREADS * K >= a.n || w.z < 0 || w.z >= a.jsplit) {
+      if (threadIdx.x == 0) raise_err(q.err, NB_DEVERR_QUEUE);
+      continue;
+    }
     if (!q.kick) a.vel = nullptr;
     ap_item<THREADS, K>(a, w.y, w.z, s_tile, s_bar, &s_last, tc);
   }
@@ -464,6 +472,8 @@ int launch_ens_allpairs(const EnsArgs& e, const EnsAllPairs& ap, cudaStream_t st
     q.items = ap.d_items + g.first_item;
     q.nitems = g.nitems;
     q.counter = ap.d_counter + gi;
+    q.nsims = (int)ap.args.size();
+    q.err = e.err;
     q.kick = e.kick_after ? 1 : 0;
     // persistent: about two CTAs of 256 threads per SM, no more than items
     const int grid = std::min(g.nitems, sms * (g.threads == 128 ? 4 : 2));

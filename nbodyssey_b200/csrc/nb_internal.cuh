@@ -214,6 +214,8 @@ struct APQueue {
   int nitems;
   int* counter;           // next item; zeroed before the launch
   int kick;               // closing kick of the simulations that step
+  int nsims;              // entries of `sims`
+  unsigned* err;          // NB_DEVERR_QUEUE: an item out of range (skipped)
 };
 
 // all-pairs launch geometry
