@@ -230,6 +230,9 @@ int measure(nb_tune_table* t) {
     const int n = 1 << (9 + bk);
     NB_TRY(b.load(n));
     StepArgs a = b.args(n, 0.5f, NB_TRAVERSE_WARP);
+    // the packed sources' buffer (and the workspace's basics) before the
+    // prep kernel writes them
+    NB_TRY(ws_reserve_allpairs(b.w, n, allpairs_geometry_for(n, 256, 4, 8 * sms)));
     NB_TRY(launch_prep(b.w, a, false, true, b.st));   // packed sources
     double best = 1e30;
     for (auto& sh : shapes)
