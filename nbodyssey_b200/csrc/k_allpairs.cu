@@ -376,7 +376,8 @@ size_t ap_region_f4(int n) {
 }
 
 size_t plan_ens_allpairs(const SimDesc* sims, int nsims, const size_t* region_of,
-                         EnsAllPairs& ap) {
+                         EnsAllPairs& ap, const size_t* region_cap, int* too_small) {
+  if (too_small) *too_small = 0;
   ap.args.clear();
   ap.sim.clear();
   ap.region.clear();
@@ -401,6 +402,10 @@ size_t plan_ens_allpairs(const SimDesc* sims, int nsims, const size_t* region_of
     a.half_dt = d.half_dt;
     const size_t r = region_of ? region_of[s] : next;
     next = r + ap_region_f4(d.n);
+    if (region_cap && ap_region_f4(d.n) > region_cap[s]) {   // the table changed
+      if (too_small) ++*too_small;
+      continue;
+    }
     top = std::max(top, next);
     ap.src_off[s] = (int)r;
     todo.push_back({(int)ap.args.size(), g});

@@ -358,9 +358,13 @@ struct EnsAllPairs {
 size_t ap_region_f4(int n);
 // Host plan of the simulations whose SimDesc.force is NB_FORCE_NAIVE and that
 // are active: geometry, items, and the region of simulation s at
-// region_of[s] (nullptr: back to back from 0).  Returns the pool size used.
+// region_of[s] (nullptr: back to back from 0).  With region_cap, a simulation
+// whose geometry now needs more than region_cap[s] float4 (the tuning table
+// changed since its region was sized) is left out and counted in *too_small.
+// Returns the pool size used.
 size_t plan_ens_allpairs(const SimDesc* sims, int nsims, const size_t* region_of,
-                         EnsAllPairs& ap);
+                         EnsAllPairs& ap, const size_t* region_cap = nullptr,
+                         int* too_small = nullptr);
 // Points the per-simulation arguments at the batch's arrays and the pool and
 // uploads them with the items and source offsets (stream-ordered; the host
 // vectors must live until the copies ran).

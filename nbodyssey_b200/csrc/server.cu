@@ -98,6 +98,7 @@ struct nb_server {
   int ap_chunks = 0;
   std::map<int, int> ap_free;        // start chunk -> length
   std::vector<size_t> ap_region;     // by sim id: region offset (float4)
+  std::vector<size_t> ap_region_cap; // by sim id: region size (float4)
   EnsAllPairs ap;
   size_t ap_items_cap = 0;
   bool any_tree = false;
@@ -310,6 +311,7 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
     d.compensated = r->p.compensated ? 1 : 0;
     d.force = r->force;
     s->ap_region[id] = r->ap_chunk >= 0 ? (size_t)r->ap_chunk * kApChunk : 0;
+    s->ap_region_cap[id] = r->ap_chunk >= 0 ? (size_t)r->ap_len * kApChunk : 0;
     for (int b = 0; b < nb32; ++b) s->blk[b0 + b] = id;
     s->table_dirty = true;
     s->running.push_back(r);
@@ -349,7 +351,12 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
       NB_CUDA(cudaMemcpyAsync((void*)s->e.runs, s->plan.runs.data(),
                               sizeof(BuildRun) * s->plan.runs.size(),
                               cudaMemcpyHostToDevice, s->stream));
-    plan_ens_allpairs(s->sims.data(), nsims, s->ap_region.data(), s->ap);
+    int too_small = 0;
+    plan_ens_allpairs(s->sims.data(), nsims, s->ap_region.data(), s->ap,
+                      s->ap_region_cap.data(), &too_small);
+    if (too_small)
+      return set_error(NB_ERR_STATE, "the tuning table changed while all-pairs requests "
+                                     "were running: their scratch no longer fits");
     if (s->ap.items.size() > s->ap_items_cap) {   // grow-only, rare
       NB_CUDA(cudaStreamSynchronize(s->stream));
       if (s->ap.d_items) cudaFree(s->ap.d_items);
@@ -562,6 +569,7 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
   }
   s->sims.assign(max_sims, SimDesc{});
   s->ap_region.assign(max_sims, 0);
+  s->ap_region_cap.assign(max_sims, 0);
   s->blk.assign(s->cap_slots / 32, -1);
   s->free_blocks[0] = s->cap_slots / 32;
   if (s->ap_chunks > 0) s->ap_free[0] = s->ap_chunks;
