@@ -69,9 +69,13 @@ typedef struct nb_params {
                           63 (21 bits/axis, the reference's width) */
   int32_t compensated; /* 1: positions kept as a hi/lo float pair through the
                           drift (forces use hi); 0: plain float drift */
-  int32_t walk_kernel; /* 0: batched list walk (default); 1: depth-first walk,
-                          one node visit per step as the reference kernels.
-                          Both give the same interaction sets. */
+  int32_t walk_kernel; /* 0: pair walk (default: a lane decides both children
+                          of an opened node from its child-pair record);
+                          1: depth-first walk, one node visit per step as the
+                          reference kernels; 2: list walk (one candidate node
+                          per lane); 3: pair walk reading the children from
+                          the node records.  All give the same interaction
+                          sets. */
 } nb_params;
 
 /* Fills the reference defaults: dt 0.01, eps 0.05, G 1, theta 0.5, naive,

@@ -105,8 +105,18 @@ __device__ __forceinline__ float box_far2(float cx, float cy, float cz, float lo
   return fx * fx + fy * fy + fz * fz;
 }
 
+// Stack word of an opened node read from its Node record (NODES walks): its
+// split (the index of its left child) and whether each child is a leaf.
+__device__ __forceinline__ int node_word(int left, int right, int ni) {
+  const unsigned sc = (unsigned)(left < ni ? left : left - ni);
+  return (int)(sc | (left >= ni ? 1u << 30 : 0u) | (right >= ni ? 1u << 31 : 0u));
+}
+
 // The walk of warp `wg` (targets 32wg .. 32wg+31); all 32 lanes call it.
-template <int W, bool MASKED, bool COUNT, bool HOIST = false>
+// NODES: the children of an opened node come from the Node records (node or
+// leaf k and k + 1 for the node that splits after leaf k) instead of its
+// child-pair record.
+template <int W, bool MASKED, bool COUNT, bool HOIST = false, bool NODES = false>
 __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
                                                PairSmem<W, MASKED>& sm) {
   const unsigned full = 0xffffffffu;
@@ -198,7 +208,8 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     const Node root = a.nodes[0];
     const bool acc = accepts(root.size2, theta2, root.com.x, root.com.y, root.com.z,
                              bi.x, bi.y, bi.z);
-    const int sc0 = root.left < ni ? root.left : root.left - ni;
+    const int sc0 = NODES ? node_word(root.left, root.right, ni)
+                          : (root.left < ni ? root.left : root.left - ni);
     const unsigned am = MASKED ? (__ballot_sync(full, acc) & live_mask)
                                : (__all_sync(full, acc) ? live_mask : 0u);
     if (lane == 0) {
@@ -233,13 +244,50 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     }
     __syncwarp();
     sp = base;
-    k = min(max(k, 0), ni - 1);   // a valid tree never needs the clamp
     float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
-    if (has) {
-      const PairRec* r = a.pairs + k;
-      A = r->a;
-      B = r->b;
-      C = r->c;
+    bool in0, in1;   // child is an internal node
+    if (NODES) {
+      const unsigned wd = (unsigned)k;
+      const int sc = (int)(wd & 0x3fffffffu);
+      const bool lf0 = (wd >> 30) & 1u, lf1 = wd >> 31;
+      // a valid tree never needs the clamps
+      const int i0 = min(sc, lf0 ? n - 1 : ni - 1), i1 = min(sc + 1, lf1 ? n - 1 : ni - 1);
+      float4 c0 = A, c1 = A;
+      float s0 = -1.f, s1 = -1.f;
+      int w0n = -1, w1n = -1;
+      if (has) {
+        if (lf0) {
+          c0 = a.ps[i0];
+        } else {
+          const Node d0 = a.nodes[i0];
+          c0 = d0.com;
+          s0 = d0.size2;
+          w0n = node_word(d0.left, d0.right, ni);
+        }
+        if (lf1) {
+          c1 = a.ps[i1];
+        } else {
+          const Node d1 = a.nodes[i1];
+          c1 = d1.com;
+          s1 = d1.size2;
+          w1n = node_word(d1.left, d1.right, ni);
+        }
+      }
+      A = make_float4(c0.x, c1.x, c0.y, c1.y);
+      B = make_float4(c0.z, c1.z, c0.w, c1.w);
+      C = make_float4(s0, s1, __int_as_float(w0n), __int_as_float(w1n));
+      in0 = !lf0;
+      in1 = !lf1;
+    } else {
+      k = min(max(k, 0), ni - 1);   // a valid tree never needs the clamp
+      if (has) {
+        const PairRec* r = a.pairs + k;
+        A = r->a;
+        B = r->b;
+        C = r->c;
+      }
+      in0 = __float_as_int(C.z) >= 0;
+      in1 = __float_as_int(C.w) >= 0;
     }
     // child 0 = (A.x, A.z, B.x) mass B.z size2 C.x split C.z; child 1 = .y/.w
     const int w0 = __float_as_int(C.z), w1 = __float_as_int(C.w);
@@ -326,7 +374,7 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       acc1 = (bacc1 || (amb1 && (r1 & live_mask) == live_mask)) ? M : 0u;
     }
     const bool ent0 = has && acc0 != 0u, ent1 = has && acc1 != 0u;
-    const bool psh0 = has && acc0 != M && w0 >= 0, psh1 = has && acc1 != M && w1 >= 0;
+    const bool psh0 = has && acc0 != M && in0, psh1 = has && acc1 != M && in1;
     const unsigned eb0 = __ballot_sync(full, ent0), eb1 = __ballot_sync(full, ent1);
     const int ne0 = __popc(eb0);
     if (ent0) {
@@ -393,10 +441,19 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
   }
 }
 
+// At most 64 registers a thread: 32 warps resident per SM whatever the block
+// shape (the compiler otherwise takes 70 for 8-warp blocks).
 template <int W, bool MASKED, bool COUNT>
-__global__ void __launch_bounds__(W * 32) k_walk_pair(WalkArgs a) {
+__global__ void __launch_bounds__(W * 32, 32 / W) k_walk_pair(WalkArgs a) {
   __shared__ PairSmem<W, MASKED> sm;
   walk_pair_warp<W, MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
+}
+
+template <int W, bool MASKED, bool COUNT>
+__global__ void __launch_bounds__(W * 32, 32 / W) k_walk_node(WalkArgs a) {
+  __shared__ PairSmem<W, MASKED> sm;
+  walk_pair_warp<W, MASKED, COUNT, false, true>(
+      a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
 }
 
 // Ensemble: each warp takes one 32-slot block of the concatenated sorted
@@ -445,15 +502,23 @@ int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
   return NB_OK;
 }
 
-template <int W>
+template <int W, bool NODES>
 static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaStream_t st) {
   if (masked) {
     // the lane masks double the stack: thread semantics stay at <= 4 warps
     // per block (<= 32 KB of static shared memory)
     constexpr int WM = W < 4 ? W : 4;
     const int bm = (blocks * W + WM - 1) / WM;
-    if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
-    else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
+    if (NODES) {
+      if (a.counts) k_walk_node<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
+      else k_walk_node<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
+    } else {
+      if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
+      else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
+    }
+  } else if (NODES) {
+    if (a.counts) k_walk_node<W, false, true><<<blocks, W * 32, 0, st>>>(a);
+    else k_walk_node<W, false, false><<<blocks, W * 32, 0, st>>>(a);
   } else {
     if (a.counts) k_walk_pair<W, false, true><<<blocks, W * 32, 0, st>>>(a);
     else k_walk_pair<W, false, false><<<blocks, W * 32, 0, st>>>(a);
@@ -461,16 +526,25 @@ static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaS
 }
 
 // The block shape (warps per block) is the tuning table's.
-int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
+template <bool NODES>
+static int launch_walk_pairs(const WalkArgs& a, bool masked, cudaStream_t st) {
   const int warps = (a.t1 - a.t0 + 31) / 32;
   if (warps <= 0) return NB_OK;
   const int W = tune_walk_warps();
   const int blocks = (warps + W - 1) / W;
-  if (W == 2) launch_walk_pair_w<2>(a, masked, blocks, st);
-  else if (W == 8) launch_walk_pair_w<8>(a, masked, blocks, st);
-  else launch_walk_pair_w<4>(a, masked, blocks, st);
+  if (W == 2) launch_walk_pair_w<2, NODES>(a, masked, blocks, st);
+  else if (W == 8) launch_walk_pair_w<8, NODES>(a, masked, blocks, st);
+  else launch_walk_pair_w<4, NODES>(a, masked, blocks, st);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
+}
+
+int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
+  return launch_walk_pairs<false>(a, masked, st);
+}
+
+int launch_walk_node(const WalkArgs& a, bool masked, cudaStream_t st) {
+  return launch_walk_pairs<true>(a, masked, st);
 }
 
 }  // namespace nb
