@@ -504,8 +504,13 @@ def served_summary(args):
             "ratio_vs_plain": srv["ratio_vs_plain"],
             "latency_s": srv["latency_s"], "accuracy": srv["accuracy"],
             "ensemble": {"workload": "128 encounters, N log-uniform [2048, 131072], "
-                                     "100 steps, force auto (%d all-pairs, crossover %d), "
-                                     "theta 0.5" % (ens["allpairs_sims"], ens["crossover"]),
+                                     "100 steps, force auto (all-pairs: %d batched below "
+                                     "%d, %d plain below %d), theta 0.5" %
+                                     (ens["allpairs_sims"]["batched"],
+                                      ens["crossover"]["batch"],
+                                      ens["allpairs_sims"]["plain"],
+                                      ens["crossover"]["alone"]),
+                         "same_module_batched": ens["same_module_batched"],
                          "value": ens["value"], "unit": "particle-steps/s",
                          "plain_fifo_particle_steps_per_s":
                              ens["plain_fifo_particle_steps_per_s"],
@@ -634,10 +639,27 @@ def ensemble_measure(nsims, steps, warmup, theta, traverse, walk, seed=0,
     dev_ms = ens.elapsed_ms(0, 1)
     for s in range(ens.nsims):
         ens.state(s)
+    batch_forces = [ens.force(s) for s in range(ens.nsims)]
     ens.close()
     wall_b = time.perf_counter() - t0
     dev_ms = dist_max(pg, dev_ms)
     wall_b = dist_max(pg, wall_b)
+
+    # batched with the module each simulation gets alone (the plain path's
+    # AUTO choice): the same arithmetic as the plain arm, bit for bit
+    from dataclasses import replace
+    tune = api.tune_get()
+    x = tune["crossover"][1][1 if traverse == "warp" else 0]
+    alone = [("naive" if force == "naive" or (force == "auto" and p.shape[0] < x) else "bh")
+             for p, _ in states]
+    ens = Ensemble(states, [replace(prm, force=f) for f in alone])
+    ens.step(W)
+    ens.sync()
+    ens.record(0)
+    ens.step(K)
+    ens.record(1)
+    same_ms = dist_max(pg, ens.elapsed_ms(0, 1))
+    ens.close()
 
     # plain path, first in first out
     dist_barrier(pg)
@@ -658,21 +680,27 @@ def ensemble_measure(nsims, steps, warmup, theta, traverse, walk, seed=0,
     wall_p = time.perf_counter() - t0
     plain_ms = dist_max(pg, plain_ms)
     wall_p = dist_max(pg, wall_p)
-    tune = api.tune_get()
-    x = tune["crossover"][1][1 if traverse == "warp" else 0]
-    n_allpairs = sum(1 for sp in specs if force == "naive" or (force == "auto" and sp["n"] < x))
     total_parts = sum(sp["n"] for sp in specs)   # all ranks' shares together
     assert world > 1 or parts == total_parts
     value = total_parts * K / (dev_ms * 1e-3)
     plain = total_parts * K / (plain_ms * 1e-3)
+    same = total_parts * K / (same_ms * 1e-3)
     return {"value": value, "unit": "particle-steps/s", "steps": K, "warmup": W,
             "ms_per_step": dev_ms / K, "particles": total_parts, "nsims": nsims,
             "plain_fifo_particle_steps_per_s": plain,
             "ratio_vs_plain_device": value / plain,
             "wall_s": {"batched": wall_b, "plain_fifo": wall_p,
                        "ratio": wall_p / wall_b},
-            "force": force, "allpairs_sims": n_allpairs,
-            "crossover": x}
+            "force": force,
+            "allpairs_sims": {"batched": batch_forces.count("naive"),
+                              "plain": alone.count("naive")},
+            "crossover": {"alone": x,
+                          "batch": tune["crossover_batch"][[0.3, 0.5, 0.7].index(
+                              min((0.3, 0.5, 0.7), key=lambda c: abs(c - theta)))]},
+            "same_module_batched": {
+                "value": same, "ratio_vs_plain_device": same / plain,
+                "note": "each simulation with the module it gets alone (results "
+                        "bit-identical to the plain arm)"}}
 
 
 def run_ensemble(args, rank, world, local, pg):
@@ -696,7 +724,11 @@ def run_ensemble(args, rank, world, local, pg):
             "plain_fifo_particle_steps_per_s": r["plain_fifo_particle_steps_per_s"],
             "ratio_vs_plain_device": r["ratio_vs_plain_device"],
             "wall_s": r["wall_s"], "allpairs_sims": r["allpairs_sims"],
-            "crossover": r["crossover"],
+            "crossover": r["crossover"], "same_module_batched": r["same_module_batched"],
+            "accuracy": "batched AUTO takes Barnes-Hut theta %.2g (median force error "
+                        "<= 1%% vs FP64) above the batch crossover where the plain "
+                        "path takes all-pairs below its own crossover; "
+                        "same_module_batched compares the same arithmetic" % args.theta,
             "gpu_launches": ENS_KERNELS_PER_STEP * r["steps"]}
     print(json.dumps(line), flush=True)
 
@@ -795,13 +827,18 @@ def serve_measure(requests, nmax, smax, budget_gb, traverse, walk, seed, smin=10
     _, lat_s, st2 = serve_all(arrivals)
     _, lat_f = fifo_all(arrivals)
     tune = api.tune_get()
-    n_ap = sum(1 for p, _, prm, _ in reqs
-               if p.shape[0] < tune["crossover"][[0.3, 0.5, 0.7].index(round(prm.theta, 1))]
-               [1 if traverse == "warp" else 0])
+    # all-pairs requests: served below the batch crossover, plain below the
+    # crossover alone (the same theta class)
+    def cls(prm):
+        return [0.3, 0.5, 0.7].index(round(prm.theta, 1))
+    n_ap = sum(1 for p, _, prm, _ in reqs if p.shape[0] < tune["crossover_batch"][cls(prm)])
+    n_ap_plain = sum(1 for p, _, prm, _ in reqs
+                     if p.shape[0] < tune["crossover"][cls(prm)][1 if traverse == "warp" else 0])
     return {"value": cap_s, "unit": "particle-steps/s",
             "workload": "%d requests, N log-uniform [4096, %d], steps U[%d, %d], theta "
-                        "{0.3,0.5,0.7}, force auto (%d all-pairs), frame every 50 steps, "
-                        "HBM budget %.0f GB" % (requests, nmax, smin, smax, n_ap, budget_gb),
+                        "{0.3,0.5,0.7}, force auto (all-pairs: %d served, %d plain), "
+                        "frame every 50 steps, HBM budget %.0f GB" %
+                        (requests, nmax, smin, smax, n_ap, n_ap_plain, budget_gb),
             "particle_steps": work,
             "plain_fifo_particle_steps_per_s": cap_f,
             "ratio_vs_plain": cap_s / cap_f,
@@ -811,8 +848,10 @@ def serve_measure(requests, nmax, smax, budget_gb, traverse, walk, seed, smin=10
             "server": {"peak_running": st["peak_running"],
                        "engine_steps": st["engine_steps"], "frames": st["frames"],
                        "frame_bytes": st["frame_bytes"]},
-            "accuracy": "equal: each request's result is bit-identical served and "
-                        "alone (tests/test_gpu_server.py)"}
+            "accuracy": "each request's result is bit-identical served and alone "
+                        "with the same module (tests/test_gpu_server.py); AUTO takes "
+                        "Barnes-Hut (median force error <= 1% vs FP64) from the batch "
+                        "crossover served, from its own crossover plain"}
 
 
 def run_serve(args, rank, world, local, pg):

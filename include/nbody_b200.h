@@ -105,13 +105,13 @@ NB_API int nb_measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
  * all-pairs / Barnes-Hut crossover NB_FORCE_AUTO uses, measured on the device
  * at first use: the first nb_sim_create / nb_ensemble_create /
  * nb_server_create on a device loads the cache file
- * ($NBODY_B200_TUNE_CACHE, else ~/.cache/nbodyssey_b200/tune_<device>_<SMs>sm_v1.bin)
+ * ($NBODY_B200_TUNE_CACHE, else ~/.cache/nbodyssey_b200/tune_<device>_<SMs>sm_v2.bin)
  * or, when there is none, measures the table (about a second) and writes
  * it.  NBODY_B200_TUNE=off keeps the defaults.  The device-pointer entry
  * points use the current table and never measure.  The shape decides only
  * the launch: the same table gives the same bits however it was obtained.
  * ==================================================================== */
-#define NB_TUNE_VERSION 1
+#define NB_TUNE_VERSION 2
 #define NB_TUNE_BUCKETS 16 /* size bucket b: n < 2^(10+b) (the last: any n) */
 #define NB_TUNE_THETAS 3   /* crossover per theta class 0.3, 0.5, 0.7 */
 typedef struct nb_tune_table {
@@ -126,6 +126,11 @@ typedef struct nb_tune_table {
   int32_t crossover[NB_TUNE_THETAS][2]; /* all-pairs below this many particles,
                                            per theta class and traversal
                                            (thread, warp) */
+  int32_t crossover_batch[NB_TUNE_THETAS]; /* the same inside a batch
+                                           (ensembles, the server): all-pairs
+                                           vs Barnes-Hut cost per particle-step
+                                           of equal-size simulations advanced
+                                           together, per theta class */
 } nb_tune_table;
 /* Measures the table on the current device and installs it; writes it to
  * cache_path when non-NULL. */
@@ -135,7 +140,8 @@ NB_API int nb_tune_get(nb_tune_table* out);
 /* Installs a table for the current device (e.g. a choice made by hand). */
 NB_API int nb_tune_set(const nb_tune_table* t);
 /* The built-in defaults for the current device: 256 x 4 all-pairs shape,
- * 8 CTAs per SM in flight, 4 walk warps per block, crossover 20,000. */
+ * 8 CTAs per SM in flight, 4 walk warps per block, crossover 20,000 alone and
+ * 4,096 in a batch. */
 NB_API int nb_tune_defaults(nb_tune_table* out);
 /* Loads / saves a cache file (NULL: the default path).  nb_tune_load fails
  * with NB_ERR_NOTFOUND for a missing file or one measured on another kind of
@@ -340,6 +346,10 @@ NB_API int nb_ensemble_get_state(nb_ensemble* e, int sim, float* pos4, float* ve
 NB_API int nb_ensemble_get_accelerations(nb_ensemble* e, int sim, float* acc4);
 /* e3[nsims][3] = {E, KE, PE} of every simulation, FP64 reductions. */
 NB_API int nb_ensemble_energy(nb_ensemble* e, double* e3);
+/* The force module simulation `sim` runs with (NB_FORCE_NAIVE or
+ * NB_FORCE_BH): NB_FORCE_AUTO resolves by the tuning table's crossover inside
+ * a batch (crossover_batch), not the one a simulation gets alone. */
+NB_API int nb_ensemble_force(const nb_ensemble* e, int sim, int* force);
 NB_API int nb_ensemble_record(nb_ensemble* e, int slot /* 0..15 */);
 NB_API int nb_ensemble_elapsed_ms(nb_ensemble* e, int slot0, int slot1, double* ms);
 
@@ -380,6 +390,9 @@ NB_API int nb_server_wait(nb_server* s, long long id, double timeout_s);
 NB_API int nb_server_result(nb_server* s, long long id, float* pos4, float* vel4,
                             int release);
 NB_API int nb_server_get_stats(nb_server* s, nb_server_stats* out);
+/* The force module request `id` runs with (NB_FORCE_NAIVE or NB_FORCE_BH;
+ * AUTO resolved by the batch crossover, as in ensembles). */
+NB_API int nb_server_force(nb_server* s, long long id, int* force);
 
 /* ======================================================================
  * Files and the run loop (src/main.cu:115-215, docs/FORMATS.md).

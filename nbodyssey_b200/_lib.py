@@ -54,7 +54,7 @@ class nb_params(ctypes.Structure):
                 ("walk_kernel", ctypes.c_int32)]
 
 
-NB_TUNE_VERSION = 1
+NB_TUNE_VERSION = 2
 NB_TUNE_BUCKETS = 16
 NB_TUNE_THETAS = 3
 
@@ -66,7 +66,8 @@ class nb_tune_table(ctypes.Structure):
                 ("ap_k", ctypes.c_int32 * NB_TUNE_BUCKETS),
                 ("ap_ctas", ctypes.c_int32 * NB_TUNE_BUCKETS),
                 ("walk_warps", ctypes.c_int32),
-                ("crossover", (ctypes.c_int32 * 2) * NB_TUNE_THETAS)]
+                ("crossover", (ctypes.c_int32 * 2) * NB_TUNE_THETAS),
+                ("crossover_batch", ctypes.c_int32 * NB_TUNE_THETAS)]
 
 
 class nb_run_stats(ctypes.Structure):
@@ -148,6 +149,7 @@ SIGNATURES = {
     "nb_ensemble_get_state": (_I, [_P, _I, _P, _P]),
     "nb_ensemble_get_accelerations": (_I, [_P, _I, _P]),
     "nb_ensemble_energy": (_I, [_P, _P]),
+    "nb_ensemble_force": (_I, [_P, _I, ctypes.POINTER(_I)]),
     "nb_ensemble_record": (_I, [_P, _I]),
     "nb_ensemble_elapsed_ms": (_I, [_P, _I, _I, ctypes.POINTER(_D)]),
     "nb_server_create": (_I, [_SZ, _I, _PP]),
@@ -159,6 +161,7 @@ SIGNATURES = {
     "nb_server_wait": (_I, [_P, ctypes.c_longlong, _D]),
     "nb_server_result": (_I, [_P, ctypes.c_longlong, _P, _P, _I]),
     "nb_server_get_stats": (_I, [_P, _P]),
+    "nb_server_force": (_I, [_P, ctypes.c_longlong, ctypes.POINTER(_I)]),
     "nb_read_ic": (_I, [_S, ctypes.POINTER(_I), _P, _P]),
     "nb_write_ic": (_I, [_S, _I, _P, _P]),
     "nb_write_frame": (_I, [_S, _I, _I, _P]),

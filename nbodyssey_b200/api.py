@@ -90,7 +90,8 @@ def tune_table_dict(t):
     return {"version": t.version, "sms": t.sms, "device": t.device.decode(),
             "ap_threads": list(t.ap_threads), "ap_k": list(t.ap_k),
             "ap_ctas": list(t.ap_ctas), "walk_warps": t.walk_warps,
-            "crossover": [list(r) for r in t.crossover]}
+            "crossover": [list(r) for r in t.crossover],
+            "crossover_batch": list(t.crossover_batch)}
 
 
 def autotune(cache_path=None):
@@ -118,6 +119,8 @@ def tune_set(table: dict):
     t.walk_warps = table["walk_warps"]
     for i in range(L.NB_TUNE_THETAS):
         t.crossover[i][:] = table["crossover"][i]
+    if "crossover_batch" in table:
+        t.crossover_batch[:] = table["crossover_batch"]
     L.check(L.load().nb_tune_set(ctypes.byref(t)))
 
 

@@ -26,6 +26,7 @@ struct nb_ensemble {
   int* d_blk = nullptr;
   BuildPlan plan;              // tree-build levels (fixed membership)
   EnsAllPairs ap;              // the all-pairs simulations' work
+  std::vector<int> force;      // resolved force module per simulation
   size_t ap_pool_f4 = 0;
   Workspace ews;               // energy scratch
   double* d_energy = nullptr;  // [nsims][6]
@@ -179,10 +180,11 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
       d.theta2 = p.theta * p.theta;
       d.active = 1;
       d.compensated = p.compensated ? 1 : 0;
-      // the module the simulation gets alone (NB_FORCE_AUTO: the tuned
-      // crossover); all-pairs simulations stay out of the tree pipeline
-      d.force = resolve_force_tuned(p.force, n[s], p.theta, p.traverse);
+      // the force module (NB_FORCE_AUTO: the tuned crossover inside a
+      // batch); all-pairs simulations stay out of the tree pipeline
+      d.force = resolve_force_batch(p.force, n[s], p.theta);
       if (d.force == NB_FORCE_BH) coff += n[s];
+      h->force.push_back(d.force);
       const int nb32 = (n[s] + 31) / 32;
       for (int k = 0; k < nb32; ++k) blk.push_back(s);
       b += nb32 * 32;
@@ -290,6 +292,13 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     return set_error(rc, keep);
   }
   *out = h;
+  return NB_OK;
+}
+
+int nb_ensemble_force(const nb_ensemble* h, int sim, int* force) {
+  if (!h || !force) return set_error(NB_ERR_INVALID, "NULL argument");
+  if (sim < 0 || sim >= h->nsims) return set_error(NB_ERR_INVALID, "simulation index out of range");
+  *force = h->force[sim];
   return NB_OK;
 }
 

@@ -245,6 +245,8 @@ int tune_walk_warps();
 int tune_crossover(float theta, int traverse);
 // resolves NB_FORCE_AUTO for n particles (other methods pass through)
 int resolve_force_tuned(int force, int n, float theta, int traverse);
+// the same for a simulation inside a batch (ensembles, the server)
+int resolve_force_batch(int force, int n, float theta);
 // first use on the current device: load the cache file or measure the table
 // (never while `st` is capturing); idempotent
 int tune_ensure(cudaStream_t st);

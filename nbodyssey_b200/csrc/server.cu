@@ -635,7 +635,7 @@ int nb_server_submit(nb_server* s, int n, const float* pos4, const float* vel4,
                                      "with 30-bit keys");
   if ((size_t)(n + 31) / 32 * 32 > (size_t)s->cap_slots)
     return set_error(NB_ERR_NOMEM, "request larger than the server's HBM budget");
-  const int force = resolve_force_tuned(p->force, n, p->theta, p->traverse);
+  const int force = resolve_force_batch(p->force, n, p->theta);
   if (force == NB_FORCE_NAIVE && ap_chunks_of(n) > s->ap_chunks)
     return set_error(NB_ERR_NOMEM, "all-pairs request larger than the server's "
                                    "all-pairs scratch (1/8 of the HBM budget)");
@@ -666,6 +666,15 @@ int nb_server_submit(nb_server* s, int n, const float* pos4, const float* vel4,
   s->waiting.push_back(r.get());
   s->all[r->id] = std::move(r);
   s->cv.notify_all();
+  return NB_OK;
+}
+
+int nb_server_force(nb_server* s, long long id, int* force) {
+  if (!s || !force) return set_error(NB_ERR_INVALID, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return set_error(NB_ERR_NOTFOUND, "unknown request id");
+  *force = it->second->force;
   return NB_OK;
 }
 

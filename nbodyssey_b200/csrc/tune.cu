@@ -39,6 +39,9 @@ constexpr int kMaxDev = 64;
 std::mutex g_mu;
 nb_tune_table g_tab[kMaxDev];
 int g_state[kMaxDev] = {};   // 0 untouched, 1 defaults or set, 2 measured / loaded
+// set while this thread measures: batches created for the measurement use the
+// table being measured and must not start another measurement
+thread_local bool g_measuring = false;
 
 const float kThetaClass[NB_TUNE_THETAS] = {0.3f, 0.5f, 0.7f};
 
@@ -66,8 +69,10 @@ void defaults(nb_tune_table* t) {
     t->ap_ctas[b] = 8 * t->sms;
   }
   t->walk_warps = 4;
-  for (int i = 0; i < NB_TUNE_THETAS; ++i)
+  for (int i = 0; i < NB_TUNE_THETAS; ++i) {
     for (int j = 0; j < 2; ++j) t->crossover[i][j] = NB_AUTO_CROSSOVER;
+    t->crossover_batch[i] = 4096;
+  }
 }
 
 bool table_ok(const nb_tune_table& t) {
@@ -76,9 +81,11 @@ bool table_ok(const nb_tune_table& t) {
     if (!allpairs_shape_compiled(t.ap_threads[b], t.ap_k[b]) || t.ap_ctas[b] < 1)
       return false;
   if (t.walk_warps != 2 && t.walk_warps != 4 && t.walk_warps != 8) return false;
-  for (int i = 0; i < NB_TUNE_THETAS; ++i)
+  for (int i = 0; i < NB_TUNE_THETAS; ++i) {
     for (int j = 0; j < 2; ++j)
       if (t.crossover[i][j] < 0) return false;
+    if (t.crossover_batch[i] < 0) return false;
+  }
   return true;
 }
 
@@ -316,6 +323,63 @@ int measure(nb_tune_table* t) {
       else x = (int)std::lround(std::sqrt((double)grid[first - 1] * grid[first]));
       t->crossover[i][tr] = x;
     }
+  install();
+  // inside a batch: ensembles of equal-size simulations (about 2M particles
+  // in all) advanced together, all-pairs against Barnes-Hut per
+  // particle-step; the crossover is the first size from which Barnes-Hut
+  // stays cheaper (the geometric mean with the size before)
+  {
+    const int bgrid[6] = {1024, 2048, 4096, 8192, 16384, 32768};
+    double ap_cost[6], bh_cost[NB_TUNE_THETAS][6];
+    for (int gi = 0; gi < 6; ++gi) {
+      const int n = bgrid[gi];
+      const int k = std::min(256, std::max(4, (1 << 21) / n));
+      std::vector<float4> one;
+      two_disks(n, one);
+      std::vector<float4> pos((size_t)k * n), vel((size_t)k * n, make_float4(0.f, 0.f, 0.f, 0.f));
+      for (int s = 0; s < k; ++s) std::copy(one.begin(), one.end(), pos.begin() + (size_t)s * n);
+      std::vector<int> ns(k, n);
+      auto cost = [&](int force, float theta, double* out) {
+        nb_params p;
+        nb_params_default(&p);
+        p.dt = 0.005f;
+        p.eps = 0.05f;
+        p.theta = theta;
+        p.force = force;
+        p.traverse = NB_TRAVERSE_WARP;
+        std::vector<nb_params> ps(k, p);
+        nb_ensemble* e = nullptr;
+        NB_TRY(nb_ensemble_create(k, ns.data(), (const float*)pos.data(),
+                                  (const float*)vel.data(), ps.data(), &e));
+        int rc = nb_ensemble_step(e, 2);
+        if (rc == NB_OK) rc = nb_ensemble_sync(e);
+        if (rc == NB_OK) rc = nb_ensemble_record(e, 0);
+        if (rc == NB_OK) rc = nb_ensemble_step(e, 3);
+        if (rc == NB_OK) rc = nb_ensemble_record(e, 1);
+        double ms = 0.0;
+        if (rc == NB_OK) rc = nb_ensemble_elapsed_ms(e, 0, 1, &ms);
+        nb_ensemble_destroy(e);
+        NB_TRY(rc);
+        *out = ms / 3.0 / ((double)k * n);
+        return NB_OK;
+      };
+      NB_TRY(cost(NB_FORCE_NAIVE, 0.5f, &ap_cost[gi]));
+      for (int i = 0; i < NB_TUNE_THETAS; ++i)
+        NB_TRY(cost(NB_FORCE_BH, kThetaClass[i], &bh_cost[i][gi]));
+    }
+    for (int i = 0; i < NB_TUNE_THETAS; ++i) {
+      int first = 6;
+      for (int gi = 6; gi-- > 0;) {
+        if (bh_cost[i][gi] < ap_cost[gi]) first = gi;
+        else break;
+      }
+      t->crossover_batch[i] =
+          first == 0 ? bgrid[0]
+                     : (first == 6 ? 2 * bgrid[5]
+                                   : (int)std::lround(std::sqrt((double)bgrid[first - 1] *
+                                                                bgrid[first])));
+    }
+  }
   NB_CUDA(cudaStreamSynchronize(b.st));
   // a measurement that ran into a device error is not kept
   unsigned e = 0;
@@ -384,7 +448,18 @@ int resolve_force_tuned(int force, int n, float theta, int traverse) {
   return n < tune_crossover(theta, traverse) ? NB_FORCE_NAIVE : NB_FORCE_BH;
 }
 
+int resolve_force_batch(int force, int n, float theta) {
+  if (force != NB_FORCE_AUTO) return force;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const nb_tune_table& t = table_locked();
+  int best = 0;
+  for (int i = 1; i < NB_TUNE_THETAS; ++i)
+    if (std::fabs(theta - kThetaClass[i]) < std::fabs(theta - kThetaClass[best])) best = i;
+  return n < t.crossover_batch[best] ? NB_FORCE_NAIVE : NB_FORCE_BH;
+}
+
 int tune_ensure(cudaStream_t st) {
+  if (g_measuring) return NB_OK;
   const int dev = current_device();
   {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -434,7 +509,9 @@ int nb_autotune(const char* cache_path_out, nb_tune_table* out) {
     g_tab[dev] = t;   // candidates are timed against the defaults elsewhere
     g_state[dev] = 1;
   }
+  g_measuring = true;
   int rc = measure(&t);
+  g_measuring = false;
   std::lock_guard<std::mutex> lk(g_mu);
   if (rc != NB_OK) {
     defaults(&g_tab[dev]);

@@ -89,6 +89,13 @@ class Ensemble:
         L.check(self._lib.nb_ensemble_energy(self._h, L.ptr(e)))
         return e
 
+    def force(self, sim):
+        """The force module simulation `sim` runs with, "naive" or "bh"
+        (AUTO resolves by the tuned crossover inside a batch)."""
+        f = ctypes.c_int()
+        L.check(self._lib.nb_ensemble_force(self._h, int(sim), ctypes.byref(f)))
+        return "naive" if f.value == L.NB_FORCE_NAIVE else "bh"
+
     def record(self, slot):
         L.check(self._lib.nb_ensemble_record(self._h, int(slot)))
 

@@ -81,6 +81,12 @@ class Server:
     def wait(self, rid, timeout_s=600.0):
         L.check(self._lib.nb_server_wait(self._h, int(rid), float(timeout_s)))
 
+    def force(self, rid):
+        """The force module request `rid` runs with, "naive" or "bh"."""
+        f = ctypes.c_int()
+        L.check(self._lib.nb_server_force(self._h, int(rid), ctypes.byref(f)))
+        return "naive" if f.value == L.NB_FORCE_NAIVE else "bh"
+
     def result(self, rid, release=True):
         if rid not in self._n:   # let the library report the unknown id
             L.check(self._lib.nb_server_result(self._h, int(rid), None, None, 0))

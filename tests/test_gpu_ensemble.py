@@ -1,6 +1,8 @@
 """GPU parity of batched ensembles: every simulation of an ensemble ends in
 exactly the state (bit for bit) it reaches when run alone through the handle
 API with the same parameters, whatever else is in the mix; energies too."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -41,7 +43,10 @@ def test_ensemble_equals_alone(forces):
         got = [ens.state(s) for s in range(ens.nsims)]
         acc = [ens.accelerations(s) for s in range(ens.nsims)]
         e_ens = ens.energy()
+        # AUTO resolves by the batch crossover: alone, the same module
+        forces_used = [ens.force(s) for s in range(ens.nsims)]
     for s, ((pos, vel), prm) in enumerate(zip(states, params)):
+        prm = dataclasses.replace(prm, force=forces_used[s])
         with api.Simulation(pos, vel, prm) as sim:
             sim.step(steps)
             p, v, a = sim.positions(), sim.velocities(), sim.compute_forces()

@@ -3,6 +3,7 @@ admitted as slots free up, run together on the device, and each result is
 bit-identical to the same request run alone through the handle API.
 Frames stream out in the reference layout; sizes beyond the budget are
 refused."""
+import dataclasses
 import os
 import threading
 import time
@@ -81,11 +82,14 @@ def test_all_pairs_and_auto_requests_identical_alone():
                 time.sleep(0.01)
         for rid in ids:
             srv.wait(rid, 120)
+        used = [srv.force(rid) for rid in ids]
         results = [srv.result(rid) for rid in ids]
         st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0
-    for (pos, vel, prm, steps), (p, v) in zip(reqs, results):
-        ap, av = _alone(pos, vel, prm, steps)
+    assert "naive" in used and "bh" in used
+    for (pos, vel, prm, steps), (p, v), f in zip(reqs, results, used):
+        # AUTO resolves by the batch crossover: alone, the same module
+        ap, av = _alone(pos, vel, dataclasses.replace(prm, force=f), steps)
         assert np.array_equal(p, ap)
         assert np.array_equal(v, av)
 

@@ -33,6 +33,8 @@ def test_measured_table_is_valid(tuned):
     for row in tuned["crossover"]:
         for x in row:
             assert 2048 <= x <= 2 * 131072
+    for x in tuned["crossover_batch"]:
+        assert 1024 <= x <= 2 * 32768
     print("tuned table:", tuned)
 
 
