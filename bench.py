@@ -80,7 +80,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--force", choices=["bh", "naive"], default="bh",
                     help="naive: time the all-pairs module instead (e.g. --n 262144)")
-    ap.add_argument("--walk", choices=["pair", "node", "list", "dfs"], default="pair",
+    ap.add_argument("--walk", choices=["pair", "list", "dfs"], default="pair",
                     help="tree-walk kernel: batched list walk or depth-first walk")
     ap.add_argument("--workload", choices=["single", "ensemble", "serve"],
                     default="single",
@@ -435,7 +435,7 @@ def run_b200(args, rank, world, local, pg):
     build_ms = sum(phases[k] for k in ("prep", "morton", "sort", "build", "com")) / calls
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
-    kernel = ({"pair": "k_walk_pair", "node": "k_walk_node", "list": "k_walk_list"}.get(
+    kernel = ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
         args.walk, "k_walk_%s" % args.traverse) if args.force == "bh" else "k_allpairs")
     traffic = profiled_traffic(kernel) if args.n == N_DEFAULT else None
     line = {

@@ -73,9 +73,7 @@ typedef struct nb_params {
                           of an opened node from its child-pair record);
                           1: depth-first walk, one node visit per step as the
                           reference kernels; 2: list walk (one candidate node
-                          per lane); 3: pair walk reading the children from
-                          the node records.  All give the same interaction
-                          sets. */
+                          per lane).  All give the same interaction sets. */
 } nb_params;
 
 /* Fills the reference defaults: dt 0.01, eps 0.05, G 1, theta 0.5, naive,
@@ -242,12 +240,11 @@ NB_API int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
                   float* size2);
 /* Debug / parity: the child-pair records of the tree built on the current
  * positions (the layout the tree walk reads), n - 1 records of 12 floats:
- * record k = (x_l, x_r, y_l, y_r, z_l, z_r, m_l, m_r, size2_l, size2_r,
- * w_l, w_r) for the two children of the internal node that splits after
- * sorted leaf k (left: node or leaf k, right: node or leaf k + 1); an
- * internal child gives its centre of mass, mass, squared box edge and split
- * (w, the bits of an int32), a leaf its position, mass, size2 = -1 and
- * w = -1. */
+ * record k = (x_l, y_l, z_l, m_l, x_r, y_r, z_r, m_r, size2_l, w_l, size2_r,
+ * w_r) for the two children of the internal node that splits after sorted
+ * leaf k (left: node or leaf k, right: node or leaf k + 1); an internal
+ * child gives its centre of mass, mass, squared box edge and split (w, the
+ * bits of an int32), a leaf its position, mass, size2 = -1 and w = -1. */
 NB_API int nb_debug_pairs(nb_sim* s, float* rec12);
 /* Debug / parity: forces with per-particle interaction counts (original
  * order; warp mode counts the warp's shared walk for every lane). */

@@ -61,9 +61,9 @@ class SimParams:
         p.traverse = L.NB_TRAVERSE_WARP if self.traverse == BhTraversal.WARP else L.NB_TRAVERSE_THREAD
         p.key_bits = int(self.key_bits)
         p.compensated = 1 if self.compensated else 0
-        if self.walk_kernel not in ("pair", "dfs", "list", "node"):
-            raise ValueError("walk_kernel must be pair, dfs, list or node")
-        p.walk_kernel = {"pair": 0, "dfs": 1, "list": 2, "node": 3}[self.walk_kernel]
+        if self.walk_kernel not in ("pair", "dfs", "list"):
+            raise ValueError("walk_kernel must be pair, dfs or list")
+        p.walk_kernel = {"pair": 0, "dfs": 1, "list": 2}[self.walk_kernel]
         return p
 
     @classmethod
@@ -75,7 +75,7 @@ class SimParams:
                    traverse=BhTraversal.WARP if p.traverse == L.NB_TRAVERSE_WARP
                    else BhTraversal.THREAD,
                    key_bits=p.key_bits, compensated=bool(p.compensated),
-                   walk_kernel={0: "pair", 1: "dfs", 2: "list", 3: "node"}[p.walk_kernel])
+                   walk_kernel={0: "pair", 1: "dfs", 2: "list"}[p.walk_kernel])
 
 
 def _rows4(a, name):

@@ -187,7 +187,7 @@ static int check_params(const nb_params* p) {
     return set_error(NB_ERR_INVALID, "traverse must be thread or warp");
   if (p->key_bits != 30 && p->key_bits != 63)
     return set_error(NB_ERR_INVALID, "key_bits must be 30 or 63");
-  if (p->walk_kernel < 0 || p->walk_kernel > 3)
+  if (p->walk_kernel < 0 || p->walk_kernel > 2)
     return set_error(NB_ERR_INVALID, "walk_kernel must be 0 or 1");
   return NB_OK;
 }

@@ -553,13 +553,8 @@ __device__ __forceinline__ void write_pair_half(const TreeView& a, int k, int si
     raise_err(a.err(), NB_DEVERR_BOUNDS);
     return;
   }
-  float* r = reinterpret_cast<float*>(&pr[k]);
-  r[side] = p.x;
-  r[2 + side] = p.y;
-  r[4 + side] = p.z;
-  r[6 + side] = p.w;
-  r[8 + side] = size2;
-  r[10 + side] = __int_as_float(w);
+  pr[k].c[side] = p;
+  reinterpret_cast<float2*>(&pr[k].sw)[side] = make_float2(size2, __int_as_float(w));
 }
 
 // Node record of internal node id over leaves [lo, hi] split after leaf sc,

@@ -97,8 +97,7 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
     return launch_walk_pair(a, s.traverse == NB_TRAVERSE_THREAD, st);
   if (s.walk_kernel == 2)
     return launch_walk_list(a, s.traverse == NB_TRAVERSE_THREAD, st);
-  if (s.walk_kernel == 3)
-    return launch_walk_node(a, s.traverse == NB_TRAVERSE_THREAD, st);
+
   int blocks = (s.t1 - s.t0 + 255) / 256;
   if (blocks == 0) return NB_OK;
   if (s.traverse == NB_TRAVERSE_WARP) {

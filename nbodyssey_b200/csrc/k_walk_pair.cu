@@ -105,18 +105,8 @@ __device__ __forceinline__ float box_far2(float cx, float cy, float cz, float lo
   return fx * fx + fy * fy + fz * fz;
 }
 
-// Stack word of an opened node read from its Node record (NODES walks): its
-// split (the index of its left child) and whether each child is a leaf.
-__device__ __forceinline__ int node_word(int left, int right, int ni) {
-  const unsigned sc = (unsigned)(left < ni ? left : left - ni);
-  return (int)(sc | (left >= ni ? 1u << 30 : 0u) | (right >= ni ? 1u << 31 : 0u));
-}
-
 // The walk of warp `wg` (targets 32wg .. 32wg+31); all 32 lanes call it.
-// NODES: the children of an opened node come from the Node records (node or
-// leaf k and k + 1 for the node that splits after leaf k) instead of its
-// child-pair record.
-template <int W, bool MASKED, bool COUNT, bool HOIST = false, bool NODES = false>
+template <int W, bool MASKED, bool COUNT, bool HOIST = false>
 __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
                                                PairSmem<W, MASKED>& sm) {
   const unsigned full = 0xffffffffu;
@@ -208,8 +198,7 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     const Node root = a.nodes[0];
     const bool acc = accepts(root.size2, theta2, root.com.x, root.com.y, root.com.z,
                              bi.x, bi.y, bi.z);
-    const int sc0 = NODES ? node_word(root.left, root.right, ni)
-                          : (root.left < ni ? root.left : root.left - ni);
+    const int sc0 = root.left < ni ? root.left : root.left - ni;
     const unsigned am = MASKED ? (__ballot_sync(full, acc) & live_mask)
                                : (__all_sync(full, acc) ? live_mask : 0u);
     if (lane == 0) {
@@ -244,66 +233,32 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     }
     __syncwarp();
     sp = base;
-    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), B = A, C = A;
-    bool in0, in1;   // child is an internal node
-    if (NODES) {
-      const unsigned wd = (unsigned)k;
-      const int sc = (int)(wd & 0x3fffffffu);
-      const bool lf0 = (wd >> 30) & 1u, lf1 = wd >> 31;
-      // a valid tree never needs the clamps
-      const int i0 = min(sc, lf0 ? n - 1 : ni - 1), i1 = min(sc + 1, lf1 ? n - 1 : ni - 1);
-      float4 c0 = A, c1 = A;
-      float s0 = -1.f, s1 = -1.f;
-      int w0n = -1, w1n = -1;
-      if (has) {
-        if (lf0) {
-          c0 = a.ps[i0];
-        } else {
-          const Node d0 = a.nodes[i0];
-          c0 = d0.com;
-          s0 = d0.size2;
-          w0n = node_word(d0.left, d0.right, ni);
-        }
-        if (lf1) {
-          c1 = a.ps[i1];
-        } else {
-          const Node d1 = a.nodes[i1];
-          c1 = d1.com;
-          s1 = d1.size2;
-          w1n = node_word(d1.left, d1.right, ni);
-        }
-      }
-      A = make_float4(c0.x, c1.x, c0.y, c1.y);
-      B = make_float4(c0.z, c1.z, c0.w, c1.w);
-      C = make_float4(s0, s1, __int_as_float(w0n), __int_as_float(w1n));
-      in0 = !lf0;
-      in1 = !lf1;
-    } else {
-      k = min(max(k, 0), ni - 1);   // a valid tree never needs the clamp
-      if (has) {
-        const PairRec* r = a.pairs + k;
-        A = r->a;
-        B = r->b;
-        C = r->c;
-      }
-      in0 = __float_as_int(C.z) >= 0;
-      in1 = __float_as_int(C.w) >= 0;
+    k = min(max(k, 0), ni - 1);   // a valid tree never needs the clamp
+    float4 c0 = make_float4(0.f, 0.f, 0.f, 0.f), c1 = c0, sw = c0;
+    if (has) {
+      const PairRec* r = a.pairs + k;
+      c0 = r->c[0];
+      c1 = r->c[1];
+      sw = r->sw;
     }
-    // child 0 = (A.x, A.z, B.x) mass B.z size2 C.x split C.z; child 1 = .y/.w
-    const int w0 = __float_as_int(C.z), w1 = __float_as_int(C.w);
-    const f2 dn = pk2(box_near2(A.x, A.z, B.x, lox, loy, loz, hix, hiy, hiz),
-                      box_near2(A.y, A.w, B.y, lox, loy, loz, hix, hiy, hiz));
+    // child j: position / centre of mass (cj.x, cj.y, cj.z), mass cj.w,
+    // size2 and split in sw (.x, .y for the left child, .z, .w the right)
+    const float s0 = sw.x, s1 = sw.z;
+    const int w0 = __float_as_int(sw.y), w1 = __float_as_int(sw.w);
+    const bool in0 = w0 >= 0, in1 = w1 >= 0;   // internal children
+    const f2 dn = pk2(box_near2(c0.x, c0.y, c0.z, lox, loy, loz, hix, hiy, hiz),
+                      box_near2(c1.x, c1.y, c1.z, lox, loy, loz, hix, hiy, hiz));
     float tn0, tn1;
     up2(mul2(pk2u(th_lo), dn), tn0, tn1);
-    const bool bacc0 = C.x < tn0, bacc1 = C.y < tn1;   // leaves: -1 < anything >= 0
+    const bool bacc0 = s0 < tn0, bacc1 = s1 < tn1;   // leaves: -1 < anything >= 0
     bool amb0, amb1, brej0 = false, brej1 = false;
     if (MASKED) {
-      const f2 df = pk2(box_far2(A.x, A.z, B.x, lox, loy, loz, hix, hiy, hiz),
-                        box_far2(A.y, A.w, B.y, lox, loy, loz, hix, hiy, hiz));
+      const f2 df = pk2(box_far2(c0.x, c0.y, c0.z, lox, loy, loz, hix, hiy, hiz),
+                        box_far2(c1.x, c1.y, c1.z, lox, loy, loz, hix, hiy, hiz));
       float tf0, tf1;
       up2(mul2(pk2u(th_hi), df), tf0, tf1);
-      brej0 = !bacc0 && C.x > tf0;
-      brej1 = !bacc1 && C.y > tf1;
+      brej0 = !bacc0 && s0 > tf0;
+      brej1 = !bacc1 && s1 > tf1;
       amb0 = has && !bacc0 && !brej0;
       amb1 = has && !bacc1 && !brej1;
     } else {
@@ -317,8 +272,8 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
         const float4 q = sm.ext[w][e];
         return accepts(s2, theta2, cx, cy, cz, q.x, q.y, q.z);
       };
-      amb0 = has && !bacc0 && ext_accepts(C.x, A.x, A.z, B.x);
-      amb1 = has && !bacc1 && ext_accepts(C.y, A.y, A.w, B.y);
+      amb0 = has && !bacc0 && ext_accepts(s0, c0.x, c0.y, c0.z);
+      amb1 = has && !bacc1 && ext_accepts(s1, c1.x, c1.y, c1.z);
     }
     // children the box and the extreme target cannot settle: staged in
     // shared memory (pairs interleaved as (cx0,cx1,cy0,cy1)(cz0,cz1,s0,s1));
@@ -332,11 +287,11 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       float* am = sm.amb[w];
       if (amb0) {
         float* p = &am[(ka0 >> 1) * 8 + (ka0 & 1)];
-        p[0] = A.x; p[2] = A.z; p[4] = B.x; p[6] = C.x;
+        p[0] = c0.x; p[2] = c0.y; p[4] = c0.z; p[6] = s0;
       }
       if (amb1) {
         float* p = &am[(ka1 >> 1) * 8 + (ka1 & 1)];
-        p[0] = A.y; p[2] = A.w; p[4] = B.y; p[6] = C.y;
+        p[0] = c1.x; p[2] = c1.y; p[4] = c1.z; p[6] = s1;
       }
       if ((na & 1) && lane == 0) {   // pad: a child every target accepts
         float* p = &am[(na >> 1) * 8 + 1];
@@ -379,12 +334,12 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     const int ne0 = __popc(eb0);
     if (ent0) {
       const int e = head + lc + __popc(eb0 & lt);
-      put_entry(ent, e, A.x, A.z, B.x, B.z);
+      put_entry(ent, e, c0.x, c0.y, c0.z, c0.w);
       if (MASKED) sm.emask[w][e & (kPRing - 1)] = acc0;
     }
     if (ent1) {
       const int e = head + lc + ne0 + __popc(eb1 & lt);
-      put_entry(ent, e, A.y, A.w, B.y, B.w);
+      put_entry(ent, e, c1.x, c1.y, c1.z, c1.w);
       if (MASKED) sm.emask[w][e & (kPRing - 1)] = acc1;
     }
     lc += ne0 + __popc(eb1);
@@ -449,12 +404,6 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_walk_pair(WalkArgs a) {
   walk_pair_warp<W, MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
 }
 
-template <int W, bool MASKED, bool COUNT>
-__global__ void __launch_bounds__(W * 32, 32 / W) k_walk_node(WalkArgs a) {
-  __shared__ PairSmem<W, MASKED> sm;
-  walk_pair_warp<W, MASKED, COUNT, false, true>(
-      a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
-}
 
 // Ensemble: each warp takes one 32-slot block of the concatenated sorted
 // arrays; blocks belong to one simulation (bases are multiples of 32), whose
@@ -502,23 +451,15 @@ int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
   return NB_OK;
 }
 
-template <int W, bool NODES>
+template <int W>
 static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaStream_t st) {
   if (masked) {
     // the lane masks double the stack: thread semantics stay at <= 4 warps
     // per block (<= 32 KB of static shared memory)
     constexpr int WM = W < 4 ? W : 4;
     const int bm = (blocks * W + WM - 1) / WM;
-    if (NODES) {
-      if (a.counts) k_walk_node<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
-      else k_walk_node<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
-    } else {
-      if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
-      else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
-    }
-  } else if (NODES) {
-    if (a.counts) k_walk_node<W, false, true><<<blocks, W * 32, 0, st>>>(a);
-    else k_walk_node<W, false, false><<<blocks, W * 32, 0, st>>>(a);
+    if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
+    else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
   } else {
     if (a.counts) k_walk_pair<W, false, true><<<blocks, W * 32, 0, st>>>(a);
     else k_walk_pair<W, false, false><<<blocks, W * 32, 0, st>>>(a);
@@ -526,25 +467,16 @@ static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaS
 }
 
 // The block shape (warps per block) is the tuning table's.
-template <bool NODES>
-static int launch_walk_pairs(const WalkArgs& a, bool masked, cudaStream_t st) {
+int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
   const int warps = (a.t1 - a.t0 + 31) / 32;
   if (warps <= 0) return NB_OK;
   const int W = tune_walk_warps();
   const int blocks = (warps + W - 1) / W;
-  if (W == 2) launch_walk_pair_w<2, NODES>(a, masked, blocks, st);
-  else if (W == 8) launch_walk_pair_w<8, NODES>(a, masked, blocks, st);
-  else launch_walk_pair_w<4, NODES>(a, masked, blocks, st);
+  if (W == 2) launch_walk_pair_w<2>(a, masked, blocks, st);
+  else if (W == 8) launch_walk_pair_w<8>(a, masked, blocks, st);
+  else launch_walk_pair_w<4>(a, masked, blocks, st);
   NB_CUDA(cudaGetLastError());
   return NB_OK;
-}
-
-int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
-  return launch_walk_pairs<false>(a, masked, st);
-}
-
-int launch_walk_node(const WalkArgs& a, bool masked, cudaStream_t st) {
-  return launch_walk_pairs<true>(a, masked, st);
 }
 
 }  // namespace nb

@@ -47,16 +47,16 @@ struct __align__(16) Node {
 // Child pairs for the tree walk, one record per split k in [0, n-2]: the two
 // children of the internal node that splits its leaves after leaf k (the left
 // child is internal node k or leaf k, the right child internal node k+1 or
-// leaf k+1), interleaved so that one lane's three 16-byte loads give packed
-// pairs: a = (x_l, x_r, y_l, y_r), b = (z_l, z_r, m_l, m_r),
-// c = (size2_l, size2_r, w_l, w_r) with (x, y, z, m) the centre of mass and
-// mass of an internal child or the position and mass of a leaf, size2 the
-// squared longest edge of an internal child's box (-1 for a leaf, which every
-// opening test accepts) and w the split of an internal child, where its own
-// children are recorded (-1 for a leaf).  The tree build writes each child's
-// half of its parent's record; the root is the one node with no record.
+// leaf k+1).  c[j] = (x, y, z, m): the centre of mass and mass of an internal
+// child, the position and mass of a leaf; sw = (size2_l, w_l, size2_r, w_r):
+// size2 the squared longest edge of an internal child's box (-1 for a leaf,
+// which every opening test accepts) and w the split of an internal child,
+// where its own children are recorded (-1 for a leaf).  The tree build writes
+// each child's half (one 16-byte and one 8-byte store) when it finishes the
+// child; the root is the one node with no record.
 struct __align__(16) PairRec {
-  float4 a, b, c;
+  float4 c[2];
+  float4 sw;
 };
 
 // Walks keep their per-warp / per-thread stacks this deep.  A radix tree over

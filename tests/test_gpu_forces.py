@@ -41,7 +41,7 @@ def bh_forces(pos, theta, traverse, bits=30, eps=EPS, walk="pair"):
     return acc[:, :3].astype(np.float64), cnt.astype(np.int64)
 
 
-@pytest.mark.parametrize("walk", ["pair", "node", "list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 @pytest.mark.parametrize("theta", [0.3, 0.5, 0.7])
 @pytest.mark.parametrize("n", [1000, 20_000, 20_001])
@@ -53,7 +53,7 @@ def test_walk_matches_oracle(n, theta, traverse, walk):
     assert_walk_close(acc, ref)
 
 
-@pytest.mark.parametrize("walk", ["pair", "node", "list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 def test_walk_matches_oracle_63bit(traverse, walk):
     pos, _ = ic.two_disks(30_000, seed=12)
@@ -63,7 +63,7 @@ def test_walk_matches_oracle_63bit(traverse, walk):
     assert_walk_close(acc, ref)
 
 
-@pytest.mark.parametrize("walk", ["pair", "node", "list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 def test_walk_1m_subsample(walk):
     """1M particles, theta 0.5 warp walk: counts of every target equal the
     oracle's (which walks only 4096 sampled warps)."""
@@ -80,7 +80,7 @@ def test_walk_1m_subsample(walk):
     assert_walk_close(acc[orig], ref_w[live])
 
 
-@pytest.mark.parametrize("walk", ["pair", "node", "list", "dfs"])
+@pytest.mark.parametrize("walk", ["pair", "list", "dfs"])
 @pytest.mark.parametrize("traverse", ["thread", "warp"])
 def test_theta0_equals_allpairs(traverse, walk):
     n = 20_000

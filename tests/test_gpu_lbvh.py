@@ -115,12 +115,9 @@ def expected_pairs(o):
                 s2 = o.size2[c]
                 cl = int(o.children[c, 0])
                 w = cl if cl < ni else cl - ni
-            rec[k, side] = x
-            rec[k, 2 + side] = y
-            rec[k, 4 + side] = z
-            rec[k, 6 + side] = m
-            rec[k, 8 + side] = s2
-            rec[k, 10 + side] = np.int32(w).view(np.float32)
+            rec[k, 4 * side: 4 * side + 4] = (x, y, z, m)
+            rec[k, 8 + 2 * side] = s2
+            rec[k, 9 + 2 * side] = np.int32(w).view(np.float32)
     return rec
 
 
