@@ -300,6 +300,10 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       __syncwarp();
       const f2 th2 = pk2(theta2, theta2);
       const f2 qx = px(), qy = py(), qz = pz();
+      // warp semantics need only "every target accepts": a vote every lane
+      // receives, kept in a warp-uniform bit mask; thread semantics need the
+      // accepting lanes, one ballot per child through shared memory
+      unsigned long long allacc = 0ull;
       for (int q = 0; q < (na + 1) >> 1; ++q) {
         const ulonglong2 U = *reinterpret_cast<const ulonglong2*>(&am[q * 8]);
         const ulonglong2 V = *reinterpret_cast<const ulonglong2*>(&am[q * 8 + 4]);
@@ -308,16 +312,28 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
         float t0, t1, z0, z1;
         up2(mul2(th2, d2), t0, t1);
         up2(V.y, z0, z1);
-        const unsigned v0 = __ballot_sync(full, z0 < t0);
-        const unsigned v1 = __ballot_sync(full, z1 < t1);
-        if (lane == 0) {
-          sm.res[w][2 * q] = v0;
-          sm.res[w][2 * q + 1] = v1;
+        if (MASKED) {
+          const unsigned v0 = __ballot_sync(full, z0 < t0);
+          const unsigned v1 = __ballot_sync(full, z1 < t1);
+          if (lane == 0) {
+            sm.res[w][2 * q] = v0;
+            sm.res[w][2 * q + 1] = v1;
+          }
+        } else {
+          // a dead lane tests a copy of live target n-1
+          const unsigned long long b0 = __all_sync(full, z0 < t0) ? 1ull : 0ull;
+          const unsigned long long b1 = __all_sync(full, z1 < t1) ? 2ull : 0ull;
+          allacc |= (b0 | b1) << (2 * q);
         }
       }
-      __syncwarp();
-      if (amb0) r0 = sm.res[w][ka0];
-      if (amb1) r1 = sm.res[w][ka1];
+      if (MASKED) {
+        __syncwarp();
+        if (amb0) r0 = sm.res[w][ka0];
+        if (amb1) r1 = sm.res[w][ka1];
+      } else {
+        r0 = (unsigned)(allacc >> ka0) & 1u;
+        r1 = (unsigned)(allacc >> ka1) & 1u;
+      }
     }
     // accepting targets of each child
     unsigned acc0, acc1;
@@ -325,8 +341,8 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
       acc0 = bacc0 ? M : (amb0 ? (r0 & M) : 0u);
       acc1 = bacc1 ? M : (amb1 ? (r1 & M) : 0u);
     } else {
-      acc0 = (bacc0 || (amb0 && (r0 & live_mask) == live_mask)) ? M : 0u;
-      acc1 = (bacc1 || (amb1 && (r1 & live_mask) == live_mask)) ? M : 0u;
+      acc0 = (bacc0 || (amb0 && r0)) ? M : 0u;
+      acc1 = (bacc1 || (amb1 && r1)) ? M : 0u;
     }
     const bool ent0 = has && acc0 != 0u, ent1 = has && acc1 != 0u;
     const bool psh0 = has && acc0 != M && in0, psh1 = has && acc1 != M && in1;
