@@ -44,8 +44,14 @@ def _ours():
     return [sys.executable, "-m", "nbodyssey_b200.galaxy_sim"]
 
 
-def _run(cmd, timeout=1800):
+_LOG_DIR = None
+
+
+def _run(cmd, timeout=1800, log=None):
     r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if _LOG_DIR and log:   # per-run logs, as gpu_bench.sh keeps in benchmarks/logs
+        with open(os.path.join(_LOG_DIR, log + ".txt"), "w") as f:
+            f.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
     if r.returncode != 0:
         raise RuntimeError("%s failed (%d): %s" % (" ".join(cmd), r.returncode,
                                                     r.stderr[-2000:]))
@@ -77,6 +83,9 @@ def main(argv=None):
                     help="sizes up to 100,000 and 150 energy steps (a smoke run)")
     a = ap.parse_args(argv)
     os.makedirs(a.out, exist_ok=True)
+    global _LOG_DIR
+    _LOG_DIR = os.path.join(a.out, "logs")
+    os.makedirs(_LOG_DIR, exist_ok=True)
     scratch = tempfile.mkdtemp(prefix="nb_gpu_bench_")
     sides = [("ours", _ours())]
     if a.ref_bin:
@@ -91,18 +100,20 @@ def main(argv=None):
             formats.write_ic(path, pos, vel)
         return path
 
-    def case(cmd, n, th, extra, steps=10):
+    def case(cmd, n, th, extra, log, steps=10):
         return _run(cmd + ["--ic", icfile(n), "--steps", str(steps),
                            "--dump-every", "1000000", "--out",
                            os.path.join(scratch, "frames"), "--energy-log",
-                           os.path.join(scratch, "e.csv"), "--theta", str(th)] + extra)
+                           os.path.join(scratch, "e.csv"), "--theta", str(th)] + extra,
+                    log=log)
 
     # 1. gates
     for name, cmd in sides:
         for tv in ("thread", "warp"):
             for th in (0.0, 0.5):
                 out = _run(cmd + ["--ic", icfile(20000), "--compare-forces", "--theta",
-                                  str(th), "--traverse", tv])
+                                  str(th), "--traverse", tv],
+                           log="%s_gate_theta%g_%s" % (name, th, tv))
                 mx, mean = compare_mean(out)
                 summary["gates"]["%s_%s_theta%g" % (name, tv, th)] = {"max": mx, "mean": mean}
                 if th == 0.0 and not (mean is not None and mean < 1e-4):
@@ -115,7 +126,8 @@ def main(argv=None):
     for n, lab, th, extra in plan:
         row = {"n": n, "method": lab, "theta": th}
         for name, cmd in sides:
-            row["%s_ms_per_call" % name] = ms_per_call(case(cmd, n, th, extra))
+            row["%s_ms_per_call" % name] = ms_per_call(
+                case(cmd, n, th, extra, "%s_%s_n%d_theta%g" % (name, lab, n, th)))
         rows.append(row)
         print(json.dumps(row), flush=True)
     summary["sweep"] = rows
@@ -134,7 +146,7 @@ def main(argv=None):
             csv = os.path.join(a.out, "energy_%s_%s.csv" % (name, lab))
             _run(cmd + ["--ic", icfile(12000), "--steps", str(steps), "--dump-every", "100",
                         "--out", os.path.join(scratch, "frames_e"),
-                        "--energy-log", csv] + extra)
+                        "--energy-log", csv] + extra, log="%s_energy_%s" % (name, lab))
             summary["energy"]["%s_%s" % (name, lab)] = final_rel_energy(csv)
     with open(os.path.join(a.out, "summary.json"), "w") as f:
         json.dump(summary, f, indent=1)
