@@ -16,8 +16,8 @@ simulation's stream, L2 flushed by a 256 MB write before every step, max over
 ranks; N ranks run N independent replicas.  `phases_ms_per_step` comes from a
 second run of K steps launched kernel by kernel with events between the
 phases (`eager_steps_per_s`).  `e2e` = the same metric through the C ABI with the state
-(pos, vel, a(x)) uploaded from pinned host memory before and downloaded after
-every step.  `roofline` = the warp walk, useful work 20 flop x per-thread-
+(pos, vel) uploaded from pinned host memory before and downloaded after every
+step (nb_step_host_state; a(x) stays on the device).  `roofline` = the warp walk, useful work 20 flop x per-thread-
 criterion interactions, against the FP32 FMA peak measured on this GPU by a
 calibration kernel.  `cpu_baseline` = the CPU oracle port (C + OpenMP) of the
 same step on this host's cores, on a sample of targets.
@@ -407,23 +407,23 @@ def run_b200(args, rank, world, local, pg):
     graph_ms = sim.elapsed_ms(0, 1)
     clk = clocks.stop() or clk
 
-    # end to end: pinned host state in, one step, state out, every step
-    # (nb_step_host; each step's inputs are the previous step's outputs),
-    # from the same starting state
+    # end to end: pinned host state (positions, velocities) in, one step,
+    # state out, every step (nb_step_host_state: a(x) stays on the device
+    # while each step's inputs are the previous step's outputs, which the
+    # library checks on the device every call), from the same starting state
     restore()
     keep = []
-    bufs = [[pinned_array(lib, (n, 4), keep) for _ in range(3)] for _ in range(2)]
+    bufs = [[pinned_array(lib, (n, 4), keep) for _ in range(2)] for _ in range(2)]
     L.check(lib.nb_get_positions(sim._h, L.ptr(bufs[0][0])))
     L.check(lib.nb_get_velocities(sim._h, L.ptr(bufs[0][1])))
-    L.check(lib.nb_get_accelerations(sim._h, L.ptr(bufs[0][2])))
     cur = 0
     for it in range(args.e2e_steps + 2):
         if it == 2:
             dist_barrier(pg)
             t0 = time.perf_counter()
         i, o = bufs[cur], bufs[cur ^ 1]
-        L.check(lib.nb_step_host(sim._h, L.ptr(i[0]), L.ptr(i[1]), L.ptr(i[2]),
-                                 L.ptr(o[0]), L.ptr(o[1]), L.ptr(o[2])))
+        L.check(lib.nb_step_host_state(sim._h, L.ptr(i[0]), L.ptr(i[1]),
+                                       L.ptr(o[0]), L.ptr(o[1])))
         cur ^= 1
     e2e_s = dist_max(pg, time.perf_counter() - t0)
     for p in keep:
@@ -461,9 +461,10 @@ def run_b200(args, rank, world, local, pg):
         "gpu_launches": ((bh_kernels_per_step(n) if args.force == "bh" else 2) + 1)
                         * args.steps,
         "e2e": {"value": world * args.e2e_steps / e2e_s, "unit": "steps/s",
-                "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 48 * n,
-                "path": "nb_step_host: pinned host pos / vel / a(x) in, one step, "
-                        "pos / vel / a(x_new) out (positions return on a second "
+                "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 32 * n,
+                "path": "nb_step_host_state: pinned host pos / vel in, a device check "
+                        "that the positions are the last ones returned (a(x) carries "
+                        "on), one step, pos / vel out (positions return on a second "
                         "stream during the tree build and walk), wall clock"},
         "roofline": {"kernel": kernel, "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",

@@ -187,6 +187,20 @@ NB_API int nb_step_host(nb_sim* s, const float* pos4, const float* vel4,
                         const float* acc4, float* pos_out4, float* vel_out4,
                         float* acc_out4);
 
+/* leapfrog_step (src/integrator.cuh:19) for callers that keep the state
+ * (positions, velocities) in host memory: uploads pos / vel, steps once, and
+ * writes the new pos / vel to the out buffers -- 64 bytes per particle
+ * across PCIe instead of nb_step_host's 96.  a(x) and the low-order position
+ * parts of the compensated drift stay on the device: they carry on when the
+ * uploaded positions are bit for bit the ones this simulation holds (those
+ * the previous call returned, checked on the device every call), so a caller
+ * that hands each call's output back gets the trajectory of nb_step; other
+ * positions start over as nb_set_state does (a(x) computed from them first).
+ * Positions return on a second stream while the tree is built and walked.
+ * Synchronous; pinned host buffers give full PCIe speed. */
+NB_API int nb_step_host_state(nb_sim* s, const float* pos4, const float* vel4,
+                              float* pos_out4, float* vel_out4);
+
 /* compute_forces (src/forces.cuh:8, src/forces.cu:68-86): a(x) for the
  * current positions into the simulation's acceleration buffer, in original
  * particle order; copied to acc4 (host, n float4, w = 0) when non-NULL. */

@@ -115,6 +115,7 @@ SIGNATURES = {
     "nb_get_accelerations": (_I, [_P, _P]),
     "nb_set_state_acc": (_I, [_P, _P, _P, _P]),
     "nb_step_host": (_I, [_P, _P, _P, _P, _P, _P, _P]),
+    "nb_step_host_state": (_I, [_P, _P, _P, _P, _P]),
     "nb_compute_forces": (_I, [_P, _P]),
     "nb_step": (_I, [_P, _I]),
     "nb_sync": (_I, [_P]),

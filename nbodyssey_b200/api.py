@@ -278,6 +278,18 @@ class Simulation:
                                        L.ptr(out[0]), L.ptr(out[1]), L.ptr(out[2])))
         return out
 
+    def step_host_state(self, pos4, vel4, out=None):
+        """One leapfrog step of host-resident (pos, vel) (nb_step_host_state):
+        a(x) and the low-order position parts stay on the device while the
+        positions handed in are the ones the previous call returned."""
+        pos4 = _rows4(pos4, "pos4")
+        vel4 = _rows4(vel4, "vel4")
+        if out is None:
+            out = tuple(np.empty_like(pos4) for _ in range(2))
+        L.check(self._lib.nb_step_host_state(self._h, L.ptr(pos4), L.ptr(vel4),
+                                             L.ptr(out[0]), L.ptr(out[1])))
+        return out
+
     def step(self, nsteps=1):
         """leapfrog_step x nsteps (asynchronous; see sync())."""
         L.check(self._lib.nb_step(self._h, int(nsteps)))

@@ -21,6 +21,26 @@ int set_error(int code, const std::string& msg) {
 }
 const char* last_error() { return g_err.c_str(); }
 
+// *diff != 0 when a and b differ in any bit (n float4 rows).
+__global__ void k_differ(const uint4* __restrict__ a, const uint4* __restrict__ b, int n,
+                         unsigned* diff) {
+  unsigned d = 0u;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint4 x = a[i], y = b[i];
+    d |= (x.x ^ y.x) | (x.y ^ y.y) | (x.z ^ y.z) | (x.w ^ y.w);
+  }
+  if (__any_sync(0xffffffffu, d != 0u) && (threadIdx.x & 31) == 0) atomicOr(diff, 1u);
+}
+
+int launch_differ(const float4* a, const float4* b, int n, unsigned* diff, cudaStream_t st) {
+  int blocks = (n + 255) / 256;
+  if (blocks > 4 * device_sm_count()) blocks = 4 * device_sm_count();
+  if (blocks < 1) blocks = 1;
+  k_differ<<<blocks, 256, 0, st>>>((const uint4*)a, (const uint4*)b, n, diff);
+  NB_CUDA(cudaGetLastError());
+  return NB_OK;
+}
+
 int device_sm_count() {
   static std::mutex mu;
   static int count[64] = {};
@@ -341,6 +361,11 @@ struct nb_sim {
   // nb_step_host: positions leave on a side stream once the drift is done
   cudaStream_t io_stream = nullptr;
   cudaEvent_t io_prep = nullptr;
+  // nb_step_host_state: uploaded positions, and whether they differ from the
+  // simulation's own
+  float4* pos_in = nullptr;
+  unsigned* d_diff = nullptr;
+  unsigned* h_diff = nullptr;   // pinned
 };
 
 static void sim_free(nb_sim* s) {
@@ -360,6 +385,9 @@ static void sim_free(nb_sim* s) {
     cudaStreamDestroy(s->io_stream);
   }
   if (s->io_prep) cudaEventDestroy(s->io_prep);
+  cudaFree(s->pos_in);
+  cudaFree(s->d_diff);
+  if (s->h_diff) cudaFreeHost(s->h_diff);
   cudaFree(s->flush_buf);
   cudaFree(s->pos);
   cudaFree(s->pos_lo);
@@ -704,6 +732,50 @@ int nb_step_host(nb_sim* s, const float* pos4, const float* vel4, const float* a
   NB_CUDA(cudaStreamSynchronize(s->io_stream));
   NB_CUDA(cudaStreamSynchronize(s->stream));
   return check_device_error(s->ws, s->stream);
+}
+
+int nb_step_host_state(nb_sim* s, const float* pos4, const float* vel4, float* pos_out4,
+                       float* vel_out4) {
+  if (!s || !pos4 || !vel4 || !pos_out4 || !vel_out4)
+    return set_error(NB_ERR_INVALID, "NULL argument");
+  if (!s->io_stream)
+    NB_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking));
+  if (!s->io_prep) NB_CUDA(cudaEventCreateWithFlags(&s->io_prep, cudaEventDisableTiming));
+  if (!s->pos_in) NB_TRY(dalloc(&s->pos_in, s->n));
+  if (!s->d_diff) NB_TRY(dalloc(&s->d_diff, 1));
+  if (!s->h_diff) NB_CUDA(cudaMallocHost((void**)&s->h_diff, sizeof(unsigned)));
+  const size_t b = sizeof(float4) * s->n;
+  cudaStream_t st = s->stream;
+  NB_CUDA(cudaMemcpyAsync(s->vel, vel4, b, cudaMemcpyHostToDevice, st));
+  NB_CUDA(cudaMemcpyAsync(s->pos_in, pos4, b, cudaMemcpyHostToDevice, st));
+  // a(x) and the low-order position parts on the device belong to the
+  // simulation's positions: they carry on when the caller hands those back
+  bool same = false;
+  if (s->primed) {
+    NB_CUDA(cudaMemsetAsync(s->d_diff, 0, sizeof(unsigned), st));
+    NB_TRY(launch_differ(s->pos_in, s->pos, s->n, s->d_diff, st));
+    NB_CUDA(cudaMemcpyAsync(s->h_diff, s->d_diff, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    NB_CUDA(cudaStreamSynchronize(st));
+    same = *s->h_diff == 0;
+  }
+  if (!same) {   // new positions: plain state, a(x) from them first
+    NB_CUDA(cudaMemcpyAsync(s->pos, s->pos_in, b, cudaMemcpyDeviceToDevice, st));
+    NB_CUDA(cudaMemsetAsync(s->pos_lo, 0, b, st));
+    NB_TRY(sim_forces(s, nullptr));
+  }
+  StepArgs a = sim_args(s);
+  a.kick_drift = true;
+  a.kick_after = true;
+  a.after_prep = s->io_prep;
+  NB_TRY(enqueue_forces(s->ws, a, s->p.force, st, nullptr));
+  // positions are final after the drift: they cross PCIe while the tree is
+  // built and walked
+  NB_CUDA(cudaStreamWaitEvent(s->io_stream, s->io_prep, 0));
+  NB_CUDA(cudaMemcpyAsync(pos_out4, s->pos, b, cudaMemcpyDeviceToHost, s->io_stream));
+  NB_CUDA(cudaMemcpyAsync(vel_out4, s->vel, b, cudaMemcpyDeviceToHost, st));
+  NB_CUDA(cudaStreamSynchronize(s->io_stream));
+  NB_CUDA(cudaStreamSynchronize(st));
+  return check_device_error(s->ws, st);
 }
 
 int nb_compute_forces(nb_sim* s, float* acc4) {

@@ -189,6 +189,9 @@ int launch_flush(void* buf, size_t bytes, cudaStream_t st);
 // Streaming multiprocessors of the current device (read once per device;
 // 148 on a B200), for grid sizes that should fill the device.
 int device_sm_count();
+// *diff becomes non-zero when the n float4 rows of a and b differ in any bit
+// (*diff zeroed by the caller)
+int launch_differ(const float4* a, const float4* b, int n, unsigned* diff, cudaStream_t st);
 int measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
 
 // Arguments of the all-pairs kernel (one simulation).

@@ -201,3 +201,29 @@ def test_step_host_equals_upload_step_download(force):
             ref.step(1)
             rp, rv, ra = ref.positions(), ref.velocities(), ref.accelerations()
     assert np.array_equal(p, rp) and np.array_equal(v, rv) and np.array_equal(a, ra)
+
+
+@pytest.mark.parametrize("force", ["bh", "naive"])
+def test_step_host_state_follows_the_device_trajectory(force):
+    """nb_step_host_state with each call's output handed back: the same
+    trajectory as nb_step on device-resident state, bit for bit (a(x) and the
+    low-order position parts carry on on the device); positions changed by
+    the caller start over as nb_set_state + nb_step."""
+    pos, vel = ic.two_disks(30_000 if force == "bh" else 4_000, seed=52)
+    prm = api.SimParams(dt=0.005, epsilon=0.05, theta=0.5, force=force,
+                        traverse="warp")
+    with api.Simulation(pos, vel, prm) as sim:
+        p, v = pos, vel
+        for _ in range(4):
+            p, v = sim.step_host_state(p, v)
+        # the caller moves one particle: a fresh start from that state
+        p2 = p.copy()
+        p2[7, 0] += 0.25
+        q, w = sim.step_host_state(p2, v)
+    with api.Simulation(pos, vel, prm) as ref:
+        ref.step(4)
+        rp, rv = ref.positions(), ref.velocities()
+        assert np.array_equal(p, rp) and np.array_equal(v, rv)
+        ref.set_state(p2, v)
+        ref.step(1)
+        assert np.array_equal(q, ref.positions()) and np.array_equal(w, ref.velocities())
