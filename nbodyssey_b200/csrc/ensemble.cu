@@ -28,6 +28,7 @@ struct nb_ensemble {
   EnsAllPairs ap;              // the all-pairs simulations' work
   std::vector<int> force;      // resolved force module per simulation
   size_t ap_pool_f4 = 0;
+  std::vector<int> walk_items[2];   // the walk queue (host copy)
   Workspace ews;               // energy scratch
   double* d_energy = nullptr;  // [nsims][6]
   bool primed = false;
@@ -224,6 +225,15 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if ((rc = ens_alloc(h, &e.err, 4)) != NB_OK) break;
     if ((rc = plan_build(sims.data(), nsims, h->plan)) != NB_OK) break;
     for (const SimDesc& d : sims) h->any_tree |= d.force == NB_FORCE_BH;
+    plan_walk_queue(sims.data(), nsims, h->walk_items);
+    for (int q = 0; q < 2; ++q) {
+      int* d_items = nullptr;
+      if ((rc = ens_alloc(h, &d_items, h->walk_items[q].size())) != NB_OK) break;
+      e.walk_items[q] = d_items;
+      e.walk_nitems[q] = (int)h->walk_items[q].size();
+    }
+    if (rc != NB_OK) break;
+    if ((rc = ens_alloc(h, &e.walk_ctr, 2)) != NB_OK) break;
     h->ap_pool_f4 = plan_ens_allpairs(sims.data(), nsims, nullptr, h->ap);
     if (!h->ap.args.empty()) {
       EnsAllPairs& ap = h->ap;
@@ -278,6 +288,10 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
                              cudaMemcpyHostToDevice, st);
       row += n[s];
     }
+    for (int q = 0; q < 2 && ce == cudaSuccess; ++q)
+      if (!h->walk_items[q].empty())
+        ce = cudaMemcpyAsync((void*)e.walk_items[q], h->walk_items[q].data(),
+                             sizeof(int) * h->walk_items[q].size(), cudaMemcpyHostToDevice, st);
     if (ce == cudaSuccess && h->ap.d_pool)
       ce = cudaMemsetAsync(h->ap.d_pool, 0, sizeof(float4) * h->ap_pool_f4, st);
     if (ce != cudaSuccess) { rc = set_error(NB_ERR_CUDA, cudaGetErrorString(ce)); break; }

@@ -34,6 +34,10 @@
 // with packed FP32 math, two entries per instruction; entries whose mask
 // excludes a lane contribute with mass 0.  A stack that would overflow hands
 // the warp to the depth-first walk of the same semantics.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "f32x2.cuh"
 #include "walk_common.cuh"
 
@@ -421,48 +425,86 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_walk_pair(WalkArgs a) {
 }
 
 
-// Ensemble: each warp takes one 32-slot block of the concatenated sorted
-// arrays; blocks belong to one simulation (bases are multiples of 32), whose
-// tree, parameters and semantics the walk uses.  Simulations with the other
-// semantics are left to the other instantiation.
+// Ensembles and the server: one persistent launch per semantics.  Its warps
+// pop 32-slot blocks of the concatenated sorted arrays from a device queue
+// (costliest simulations first, so the longest walks do not start last) and
+// walk each with that block's simulation: its tree, parameters and
+// semantics.  Blocks belong to one simulation (bases are multiples of 32).
 constexpr int kEnsW = 4;
 template <bool MASKED>
 __global__ void __launch_bounds__(kEnsW * 32) k_walk_pair_ens(EnsArgs e) {
   __shared__ PairSmem<kEnsW, MASKED> sm;
-  const int blk = blockIdx.x * kEnsW + (threadIdx.x >> 5);
-  if (blk >= e.nblocks) return;
-  const int s = e.blk_sim[blk];
-  if (s < 0) return;
-  const SimDesc d = e.sims[s];
-  if (!d.active || d.n < 2 || d.force != NB_FORCE_BH ||
-      (d.traverse == NB_TRAVERSE_THREAD) != MASKED)
-    return;
-  WalkArgs a;
-  a.n = d.n;
-  a.ps = e.pos_sorted + d.base;
-  a.perm = e.perm + d.base;
-  a.nodes = e.nodes + d.base;
-  a.pairs = e.pairs + d.base;
-  a.theta2 = d.theta2;
-  a.eps2 = d.eps2;
-  a.G = d.G;
-  a.half_dt = d.half_dt;
-  a.acc = e.acc;
-  a.vel = (e.kick_after && d.active == 1) ? e.vel : nullptr;
-  a.counts = nullptr;
-  a.perm_limit = e.nslots;
-  a.err = e.err;
-  a.t0 = 0;
-  a.t1 = d.n;
-  a.part = nullptr;
-  walk_pair_warp<kEnsW, MASKED, false, true>(a, blk - d.base / 32, sm);
+  const int lane = threadIdx.x & 31;
+  const int* items = e.walk_items[MASKED ? 1 : 0];
+  const int nitems = e.walk_nitems[MASKED ? 1 : 0];
+  int* ctr = e.walk_ctr + (MASKED ? 1 : 0);
+  for (;;) {
+    int it = 0;
+    if (lane == 0) it = atomicAdd(ctr, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= nitems) return;
+    const int blk = items[it];
+    const int s = (blk >= 0 && blk < e.nblocks) ? e.blk_sim[blk] : -1;
+    if (s < 0 || s >= e.nsims) {   // a stale or corrupt item: skipped, reported
+      if (lane == 0) raise_err(e.err, NB_DEVERR_QUEUE);
+      continue;
+    }
+    const SimDesc d = e.sims[s];
+    if (!d.active || d.n < 2 || d.force != NB_FORCE_BH ||
+        (d.traverse == NB_TRAVERSE_THREAD) != MASKED)
+      continue;
+    WalkArgs a;
+    a.n = d.n;
+    a.ps = e.pos_sorted + d.base;
+    a.perm = e.perm + d.base;
+    a.nodes = e.nodes + d.base;
+    a.pairs = e.pairs + d.base;
+    a.theta2 = d.theta2;
+    a.eps2 = d.eps2;
+    a.G = d.G;
+    a.half_dt = d.half_dt;
+    a.acc = e.acc;
+    a.vel = (e.kick_after && d.active == 1) ? e.vel : nullptr;
+    a.counts = nullptr;
+    a.perm_limit = e.nslots;
+    a.err = e.err;
+    a.t0 = 0;
+    a.t1 = d.n;
+    a.part = nullptr;
+    walk_pair_warp<kEnsW, MASKED, false, true>(a, blk - d.base / 32, sm);
+    __syncwarp();   // this warp's shared memory is free for its next block
+  }
+}
+
+void plan_walk_queue(const SimDesc* sims, int nsims, std::vector<int> items[2]) {
+  items[0].clear();
+  items[1].clear();
+  std::vector<int> order;
+  for (int s = 0; s < nsims; ++s)
+    if (sims[s].active && sims[s].n >= 2 && sims[s].force == NB_FORCE_BH) order.push_back(s);
+  auto weight = [&](int s) {   // a warp's walk grows with log n and falls with theta
+    const float th = std::max(std::sqrt(sims[s].theta2), 0.05f);
+    return std::log2((float)sims[s].n) / (th * std::sqrt(th));
+  };
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return weight(x) > weight(y); });
+  for (int s : order) {
+    const int q = sims[s].traverse == NB_TRAVERSE_THREAD ? 1 : 0;
+    const int b0 = sims[s].base / 32, nb = (sims[s].n + 31) / 32;
+    for (int b = 0; b < nb; ++b) items[q].push_back(b0 + b);
+  }
 }
 
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
-  const int blocks = (e.nblocks + kEnsW - 1) / kEnsW;
-  if (blocks == 0) return NB_OK;
-  k_walk_pair_ens<false><<<blocks, kEnsW * 32, 0, st>>>(e);
-  k_walk_pair_ens<true><<<blocks, kEnsW * 32, 0, st>>>(e);
+  NB_CUDA(cudaMemsetAsync(e.walk_ctr, 0, 2 * sizeof(int), st));
+  const int cap = device_sm_count() * 8;   // 8 resident blocks of 4 warps per SM
+  for (int q = 0; q < 2; ++q) {
+    const int n = e.walk_nitems[q];
+    if (n <= 0) continue;
+    const int blocks = std::min((n + kEnsW - 1) / kEnsW, cap);
+    if (q == 0) k_walk_pair_ens<false><<<blocks, kEnsW * 32, 0, st>>>(e);
+    else k_walk_pair_ens<true><<<blocks, kEnsW * 32, 0, st>>>(e);
+  }
   NB_CUDA(cudaGetLastError());
   return NB_OK;
 }

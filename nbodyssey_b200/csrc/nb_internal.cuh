@@ -333,6 +333,12 @@ struct EnsArgs {
   const BuildRun* runs;       // tree-build plan (all levels)
   int2* seg[2];               // open splits between build levels
   int* seg_count[2];
+  // the Barnes-Hut walk's work queue: per semantics (0 warp, 1 thread) the
+  // 32-slot blocks to walk, costliest first, and a counter each (zeroed by
+  // the launcher every step)
+  const int* walk_items[2];
+  int walk_nitems[2];
+  int* walk_ctr;
 };
 
 // All-pairs work of the simulations of a batch that use the all-pairs
@@ -387,6 +393,11 @@ int plan_build(const SimDesc* sims, int nsims, BuildPlan& plan);
 size_t plan_seg_entries(int slots, int nsims);
 int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st);
 int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
+// Host: the walk queue of a simulation table (the Barnes-Hut simulations'
+// 32-slot blocks per semantics, costliest simulation first: larger n and
+// smaller theta walk longer); items[0] / items[1] get the warp / thread
+// semantics' blocks.
+void plan_walk_queue(const SimDesc* sims, int nsims, std::vector<int> items[2]);
 
 // A view of a simulation handle's device state (defined in api.cu) for the
 // run loop in io.cu.

@@ -102,6 +102,8 @@ struct nb_server {
   EnsAllPairs ap;
   size_t ap_items_cap = 0;
   bool any_tree = false;
+  std::vector<int> walk_items[2];    // the walk queue (host copy)
+  int* d_walk_items[2] = {nullptr, nullptr};
   std::vector<int> free_ids;
   bool table_dirty = false;
   BuildPlan plan;                    // tree-build levels of the running sims
@@ -366,6 +368,15 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
       s->ap_items_cap = cap;
     }
     NB_TRY(bind_ens_allpairs(s->ap, s->sims.data(), nsims, s->e, s->stream));
+    plan_walk_queue(s->sims.data(), nsims, s->walk_items);
+    for (int q = 0; q < 2; ++q) {
+      if (!s->walk_items[q].empty())
+        NB_CUDA(cudaMemcpyAsync(s->d_walk_items[q], s->walk_items[q].data(),
+                                sizeof(int) * s->walk_items[q].size(),
+                                cudaMemcpyHostToDevice, s->stream));
+      s->e.walk_items[q] = s->d_walk_items[q];
+      s->e.walk_nitems[q] = (int)s->walk_items[q].size();
+    }
     s->table_dirty = false;
   }
   // bound the queue depth: wait for the step issued kInFlight iterations ago
@@ -491,6 +502,10 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     if ((rc = srv_alloc(s, &s->ap.d_args, (size_t)max_sims)) != NB_OK) break;
     if ((rc = srv_alloc(s, &s->ap.d_src_off, (size_t)max_sims)) != NB_OK) break;
     if ((rc = srv_alloc(s, &s->ap.d_counter, 6)) != NB_OK) break;
+    for (int q = 0; q < 2; ++q)
+      if ((rc = srv_alloc(s, &s->d_walk_items[q], slots / 32)) != NB_OK) break;
+    if (rc != NB_OK) break;
+    if ((rc = srv_alloc(s, &e.walk_ctr, 2)) != NB_OK) break;
     const size_t S = slots;
     SimDesc* dsims = nullptr;
     int* dblk = nullptr;

@@ -178,6 +178,5 @@ __device__ __forceinline__ float3 dfs_walk_warp(const WalkArgs& a, float4 bi,
 
 int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st);
 int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st);
-int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
 
 }  // namespace nb
