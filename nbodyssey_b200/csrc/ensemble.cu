@@ -155,6 +155,7 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     total += n[s];
   }
   if (slots >= (1ll << 29)) return set_error(NB_ERR_INVALID, "too many particles in total");
+  NB_TRY(warm_kernels());         // first use on this device: load the kernels
   NB_TRY(tune_ensure(nullptr));   // first use on this device: the tuning table
   nb_ensemble* h = new nb_ensemble();
   h->nsims = nsims;

@@ -675,6 +675,15 @@ static int static_scratch_address(unsigned char** out) {
   return NB_OK;
 }
 
+int warm_allpairs_kernels() {
+  return warm_fns(k_allpairs<128, 2>, k_allpairs<128, 4>, k_allpairs<128, 8>,
+                  k_allpairs<256, 2>, k_allpairs<256, 4>, k_allpairs<256, 8>,
+                  k_allpairs_queue<128, 2>, k_allpairs_queue<128, 4>,
+                  k_allpairs_queue<128, 8>, k_allpairs_queue<256, 2>,
+                  k_allpairs_queue<256, 4>, k_allpairs_queue<256, 8>, k_ens_pack,
+                  k_pack_static, k_energy_phi, k_energy_reduce);
+}
+
 }  // namespace nb
 
 extern "C" int nb_compute_forces_naive_static(int n, const float* d_pos4,

@@ -1200,4 +1200,12 @@ int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st) 
   return NB_OK;
 }
 
+int warm_lbvh_kernels() {
+  return warm_fns(k_morton<uint32_t>, k_morton<uint64_t>, k_ens_morton,
+                  k_sort_pass<uint32_t, kSortMid>, k_sort_pass<uint32_t, kSortLast>,
+                  k_sort_pass<uint64_t, kSortMid>, k_sort_pass<uint64_t, kSortLast>,
+                  k_sort_pass<uint64_t, kSortLastEnsemble>, k_build_level<uint32_t, true>,
+                  k_build_level<uint64_t, true>, k_build_level<uint32_t, false>);
+}
+
 }  // namespace nb

@@ -413,4 +413,14 @@ int measure_fp32_peak(double* scalar, double* packed) {
   return NB_OK;
 }
 
+int warm_prep_kernels() {
+  return warm_fns(k_prep<true, true, true, true>, k_prep<true, true, true, false>,
+                  k_prep<true, true, false, true>, k_prep<true, true, false, false>,
+                  k_prep<true, false, true, true>, k_prep<true, false, true, false>,
+                  k_prep<true, false, false, true>, k_prep<true, false, false, false>,
+                  k_prep<false, false, true, true>, k_prep<false, false, true, false>,
+                  k_prep<false, false, false, true>, k_prep<false, false, false, false>,
+                  k_ens_prep<false>, k_ens_prep<true>);
+}
+
 }  // namespace nb

@@ -111,4 +111,11 @@ int launch_walk(Workspace& w, const StepArgs& s, cudaStream_t st) {
   return NB_OK;
 }
 
+int warm_walk_kernels() {
+  NB_TRY(warm_walk_pair_kernels());
+  NB_TRY(warm_walk_list_kernels());
+  return warm_fns(k_walk_thread<false>, k_walk_thread<true>, k_walk_warp<false>,
+                  k_walk_warp<true>, k_gather_part);
+}
+
 }  // namespace nb

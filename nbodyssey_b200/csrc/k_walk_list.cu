@@ -392,4 +392,9 @@ int launch_walk_list(const WalkArgs& a, bool masked, cudaStream_t st) {
   return NB_OK;
 }
 
+int warm_walk_list_kernels() {
+  return warm_fns(k_walk_list<false, false>, k_walk_list<false, true>,
+                  k_walk_list<true, false>, k_walk_list<true, true>);
+}
+
 }  // namespace nb

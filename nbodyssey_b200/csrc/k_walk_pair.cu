@@ -537,4 +537,13 @@ int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
   return NB_OK;
 }
 
+int warm_walk_pair_kernels() {
+  return warm_fns(k_walk_pair<2, false, false>, k_walk_pair<2, false, true>,
+                  k_walk_pair<4, false, false>, k_walk_pair<4, false, true>,
+                  k_walk_pair<8, false, false>, k_walk_pair<8, false, true>,
+                  k_walk_pair<2, true, false>, k_walk_pair<2, true, true>,
+                  k_walk_pair<4, true, false>, k_walk_pair<4, true, true>,
+                  k_walk_pair_ens<false>, k_walk_pair_ens<true>);
+}
+
 }  // namespace nb

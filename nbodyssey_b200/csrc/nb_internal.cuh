@@ -156,7 +156,7 @@ struct StepArgs {
   float eps2, G, theta2;
   int key_bits;
   int traverse;
-  int walk_kernel;  // 0 list walk, 1 depth-first walk
+  int walk_kernel;  // 0 pair walk, 1 depth-first walk, 2 list walk
   bool kick_drift;  // opening kick + drift before the force evaluation
   bool kick_after;  // closing kick fused into the force epilogue
   int* counts;      // debug: interactions per sorted target, or nullptr
@@ -193,6 +193,37 @@ int device_sm_count();
 // (*diff zeroed by the caller)
 int launch_differ(const float4* a, const float4* b, int n, unsigned* diff, cudaStream_t st);
 int measure_fp32_peak(double* tflops_scalar, double* tflops_packed);
+
+// Kernel warm-up.  With lazy module loading (the CUDA 12 default) a kernel's
+// code is loaded at its first launch, a host stall of up to milliseconds that
+// a stream's timing events then count as device time.  warm_kernels() loads
+// every kernel of the force-and-step path on the current device once per
+// process (the handle query loads the function); the first simulation,
+// ensemble or server created on a device calls it.  warm_fn queries one
+// kernel; each source file lists its own kernels.
+template <typename F>
+inline int warm_fn(F* kernel) {
+  cudaFuncAttributes fa;
+  const cudaError_t e = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(kernel));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(NB_ERR_CUDA, std::string("loading a kernel: ") + cudaGetErrorString(e));
+  }
+  return NB_OK;
+}
+inline int warm_fns() { return NB_OK; }
+template <typename F, typename... R>
+inline int warm_fns(F* kernel, R*... rest) {
+  NB_TRY(warm_fn(kernel));
+  return warm_fns(rest...);
+}
+int warm_kernels();
+int warm_prep_kernels();
+int warm_lbvh_kernels();
+int warm_walk_kernels();   // calls the two below
+int warm_walk_pair_kernels();
+int warm_walk_list_kernels();
+int warm_allpairs_kernels();
 
 // Arguments of the all-pairs kernel (one simulation).
 struct APArgs {

@@ -488,6 +488,7 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
   size_t slots = (hbm_budget_bytes - ap_bytes) / kBytesPerSlot / 4096 * 4096;
   if (slots < 4096) return set_error(NB_ERR_INVALID, "HBM budget too small");
   if (slots > ((size_t)1 << 28)) slots = (size_t)1 << 28;
+  NB_TRY(warm_kernels());         // first use on this device: load the kernels
   NB_TRY(tune_ensure(nullptr));   // first use on this device: the tuning table
   nb_server* s = new nb_server();
   s->budget = hbm_budget_bytes;
