@@ -46,9 +46,13 @@ METRIC = ("steps/s at 1M (BH θ=0.5); served particle-steps/s + p99 vs "
           "plain, equal error")
 N_DEFAULT = 1_000_000
 FLOP_PER_PAIR = 20          # src/main.cu:203-207 convention
-BUILD_BYTES_PER_PARTICLE = 230   # algorithmic HBM bytes of the tree build
+# algorithmic HBM bytes per particle of the step before the walk: kick, drift
+# and box 112 (r pos, lo, vel, acc; w pos, lo, vel), Morton keys 24, four
+# sort passes 64, sorted-position gather 32, first build level 68 (r keys,
+# sorted positions; w two 24-byte child-pair halves per particle)
+BUILD_BYTES_PER_PARTICLE = 300
+HBM_FALLBACK_GBS = 6650.0   # copy bandwidth measured on this pool's B200s (no peaks file)
 L2_FLUSH_BYTES = 256 << 20
-ENS_KERNELS_PER_STEP = 11   # prep, morton, 5 sort passes, karras, com, 2 walks
 
 
 def bh_kernels_per_step(n, key_bits=30):
@@ -439,6 +443,9 @@ def run_b200(args, rank, world, local, pg):
     build_ms = sum(phases[k] for k in ("prep", "morton", "sort", "build", "com")) / calls
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs")
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    if not hbm:   # the copy bandwidth measured earlier on this pool's B200s
+        hbm, hbm_src = HBM_FALLBACK_GBS, "6,650 GB/s copy bandwidth (of fallback)"
     kernel = ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
         args.walk, "k_walk_%s" % args.traverse) if args.force == "bh" else "k_allpairs")
     traffic = profiled_traffic(kernel) if args.n == N_DEFAULT else None
@@ -479,10 +486,10 @@ def run_b200(args, rank, world, local, pg):
                            BUILD_BYTES_PER_PARTICLE * n / (build_ms * 1e-3) / 1e9,
                            "peak": hbm, "unit": "GB/s",
                            "frac": (BUILD_BYTES_PER_PARTICLE * n / (build_ms * 1e-3) / 1e9
-                                    / hbm) if hbm else None,
-                           "work": "230 B/particle (bbox, keys, 4 sort passes, "
-                                   "gather, build, centres of mass)",
-                           "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                                    / hbm),
+                           "work": "300 B/particle (kick, drift and box 112, keys 24, "
+                                   "4 sort passes 64, gather 32, child-pair records 68)",
+                           "peak_source": hbm_src},
         "clocks": clk,
     }
     if args.force == "naive":
@@ -645,6 +652,7 @@ def ensemble_measure(nsims, steps, warmup, theta, traverse, walk, seed=0,
     for s in range(ens.nsims):
         ens.state(s)
     batch_forces = [ens.force(s) for s in range(ens.nsims)]
+    kernels = ens.kernels_per_step()
     ens.close()
     wall_b = time.perf_counter() - t0
     dev_ms = dist_max(pg, dev_ms)
@@ -696,7 +704,7 @@ def ensemble_measure(nsims, steps, warmup, theta, traverse, walk, seed=0,
             "ratio_vs_plain_device": value / plain,
             "wall_s": {"batched": wall_b, "plain_fifo": wall_p,
                        "ratio": wall_p / wall_b},
-            "force": force,
+            "force": force, "kernels_per_step": kernels,
             "allpairs_sims": {"batched": batch_forces.count("naive"),
                               "plain": alone.count("naive")},
             "crossover": {"alone": x,
@@ -734,7 +742,7 @@ def run_ensemble(args, rank, world, local, pg):
                         "<= 1%% vs FP64) above the batch crossover where the plain "
                         "path takes all-pairs below its own crossover; "
                         "same_module_batched compares the same arithmetic" % args.theta,
-            "gpu_launches": ENS_KERNELS_PER_STEP * r["steps"]}
+            "gpu_launches": r["kernels_per_step"] * r["steps"]}
     print(json.dumps(line), flush=True)
 
 

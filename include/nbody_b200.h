@@ -361,6 +361,10 @@ NB_API int nb_ensemble_energy(nb_ensemble* e, double* e3);
  * NB_FORCE_BH): NB_FORCE_AUTO resolves by the tuning table's crossover inside
  * a batch (crossover_batch), not the one a simulation gets alone. */
 NB_API int nb_ensemble_force(const nb_ensemble* e, int sim, int* force);
+/* Kernel launches of one ensemble step (prep, the tree pipeline when some
+ * simulation uses Barnes-Hut, the all-pairs packing and queue launches when
+ * some uses all-pairs). */
+NB_API int nb_ensemble_kernels_per_step(const nb_ensemble* e, int* kernels);
 NB_API int nb_ensemble_record(nb_ensemble* e, int slot /* 0..15 */);
 NB_API int nb_ensemble_elapsed_ms(nb_ensemble* e, int slot0, int slot1, double* ms);
 

@@ -151,6 +151,7 @@ SIGNATURES = {
     "nb_ensemble_get_accelerations": (_I, [_P, _I, _P]),
     "nb_ensemble_energy": (_I, [_P, _P]),
     "nb_ensemble_force": (_I, [_P, _I, ctypes.POINTER(_I)]),
+    "nb_ensemble_kernels_per_step": (_I, [_P, ctypes.POINTER(_I)]),
     "nb_ensemble_record": (_I, [_P, _I]),
     "nb_ensemble_elapsed_ms": (_I, [_P, _I, _I, ctypes.POINTER(_D)]),
     "nb_server_create": (_I, [_SZ, _I, _PP]),

@@ -133,7 +133,7 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_TRY(dalloc(&w.vals_alt, cap));
   NB_TRY(dalloc(&w.pos_sorted, cap));
   NB_TRY(dalloc(&w.nodes, ni));
-  NB_TRY(dalloc(&w.pairs, ni));
+  NB_TRY(dalloc(&w.pairs, (size_t)cap));
   NB_TRY(dalloc(&w.parent, 2 * (size_t)cap));
   for (int i = 0; i < 2; ++i) {
     NB_TRY(dalloc(&w.seg[i], build_seg_entries(cap)));
@@ -148,7 +148,7 @@ int ws_reserve(Workspace& w, int n, int key_bits) {
   NB_CUDA(cudaMemset(w.vals_alt, 0, cap * sizeof(uint32_t)));
   NB_CUDA(cudaMemset(w.parent, 0xff, 2 * (size_t)cap * sizeof(int)));
   NB_CUDA(cudaMemset(w.nodes, 0, ni * sizeof(Node)));
-  NB_CUDA(cudaMemset(w.pairs, 0, ni * sizeof(PairRec)));
+  NB_CUDA(cudaMemset(w.pairs, 0, (size_t)cap * sizeof(PairRec)));
   w.status_tiles = (cap + kSortTile - 1) / kSortTile;
   size_t words = 8 * kSortRadix + 8 + (size_t)8 * w.status_tiles * kSortRadix;
   NB_TRY(dalloc(&w.hist, words));
@@ -934,6 +934,7 @@ int nb_debug_lbvh(nb_sim* s, uint64_t* keys_sorted, uint32_t* perm,
   float4* tmp = nullptr;
   NB_TRY(dalloc(&tmp, s->n));
   a.acc = tmp;   // leave the simulation's a(x) untouched
+  a.node_records = true;
   int rc = enqueue_forces(s->ws, a, NB_FORCE_BH, s->stream, nullptr);
   if (rc == NB_OK) {
     cudaStream_t st = s->stream;

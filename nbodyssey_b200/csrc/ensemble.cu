@@ -210,9 +210,7 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if ((rc = ens_alloc(h, &e.keys_alt, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.perm, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.perm_alt, S)) != NB_OK) break;
-    if ((rc = ens_alloc(h, &e.nodes, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.pairs, S)) != NB_OK) break;
-    if ((rc = ens_alloc(h, &e.parent, 2 * S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.sums, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.box_lo, S)) != NB_OK) break;
     if ((rc = ens_alloc(h, &e.box_hi, S)) != NB_OK) break;
@@ -266,8 +264,6 @@ int nb_ensemble_create(int nsims, const int* n, const float* pos4,
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.acc, 0, S * 16, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.perm, 0, S * 4, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.perm_alt, 0, S * 4, st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(e.parent, 0xff, 2 * S * 4, st);
-    if (ce == cudaSuccess) ce = cudaMemsetAsync(e.nodes, 0, S * sizeof(Node), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.pairs, 0, S * sizeof(PairRec), st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.hist, 0, words * 4, st);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(e.err, 0, 16, st);
@@ -314,6 +310,18 @@ int nb_ensemble_force(const nb_ensemble* h, int sim, int* force) {
   if (!h || !force) return set_error(NB_ERR_INVALID, "NULL argument");
   if (sim < 0 || sim >= h->nsims) return set_error(NB_ERR_INVALID, "simulation index out of range");
   *force = h->force[sim];
+  return NB_OK;
+}
+
+int nb_ensemble_kernels_per_step(const nb_ensemble* h, int* kernels) {
+  if (!h || !kernels) return set_error(NB_ERR_INVALID, "NULL argument");
+  int k = 1;   // prep
+  if (h->any_tree) {
+    k += 1 + ens_sort_passes() + h->plan.levels;   // Morton keys, sort, build levels
+    for (int q = 0; q < 2; ++q) k += h->walk_items[q].empty() ? 0 : 1;
+  }
+  if (!h->ap.groups.empty()) k += 1 + (int)h->ap.groups.size();   // pack + queues
+  *kernels = k;
   return NB_OK;
 }
 

@@ -47,6 +47,8 @@ __global__ void __launch_bounds__(kMortonThreads) k_morton(const float4* __restr
                                                 int n, const int* __restrict__ bbox,
                                                 K* keys, uint32_t* vals,
                                                 uint32_t* hist, int passes) {
+  chain_release();
+  chain_wait();
   __shared__ uint32_t s_hist[8 * kSortRadix];
   for (int i = threadIdx.x; i < passes * kSortRadix; i += blockDim.x) s_hist[i] = 0;
   __syncthreads();
@@ -99,15 +101,12 @@ int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
   const int sms = device_sm_count();
   if (blocks > sms) blocks = sms;   // one CTA per SM: fewer histogram flushes
   if (a.key_bits == 63)
-    k_morton<uint64_t><<<blocks, kMortonThreads, 0, st>>>(a.pos, a.n, w.bbox,
-                                               (uint64_t*)w.keys, w.vals, w.hist,
-                                               passes);
-  else
-    k_morton<uint32_t><<<blocks, kMortonThreads, 0, st>>>(a.pos, a.n, w.bbox,
-                                               (uint32_t*)w.keys, w.vals, w.hist,
-                                               passes);
-  NB_CUDA(cudaGetLastError());
-  return NB_OK;
+    return launch_chained(k_morton<uint64_t>, blocks, kMortonThreads, 0, st,
+                          (const float4*)a.pos, a.n, (const int*)w.bbox,
+                          (uint64_t*)w.keys, w.vals, w.hist, passes);
+  return launch_chained(k_morton<uint32_t>, blocks, kMortonThreads, 0, st,
+                        (const float4*)a.pos, a.n, (const int*)w.bbox, (uint32_t*)w.keys,
+                        w.vals, w.hist, passes);
 }
 
 // ---------------------------------------------------------------------------
@@ -176,6 +175,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
   K* s_key = reinterpret_cast<K*>(s_stage);
   uint32_t* s_val = reinterpret_cast<uint32_t*>(s_key + kSortTile);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  chain_release();
+  chain_wait();
   if (tid == 0) s_tile = (int)atomicAdd(tile_ctr, 1u);
   for (int i = tid; i < W * kSortRadix; i += kSortThreads) (&s_wc[0][0])[i] = 0u;
 
@@ -368,10 +369,14 @@ static int launch_sort_pass(int tiles, cudaStream_t st, const K* kin, const uint
                             K* kout, uint32_t* vout, int n, int shift,
                             const uint32_t* hist, uint32_t* status, uint32_t* ctr,
                             unsigned* err, const float4* pos, float4* pos_sorted,
-                            const SimDesc* sims, int nsims) {
+                            const SimDesc* sims, int nsims, bool chained = false) {
   const int smem = kSortTile * (int)(sizeof(K) + sizeof(uint32_t));
   NB_CUDA(cudaFuncSetAttribute(k_sort_pass<K, MODE>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (chained)
+    return launch_chained(k_sort_pass<K, MODE>, tiles, kSortThreads, smem, st, kin, vin, kout,
+                          vout, n, shift, hist, status, ctr, err, pos, pos_sorted, sims,
+                          nsims);
   k_sort_pass<K, MODE><<<tiles, kSortThreads, smem, st>>>(
       kin, vin, kout, vout, n, shift, hist, status, ctr, err, pos, pos_sorted, sims, nsims);
   NB_CUDA(cudaGetLastError());
@@ -393,11 +398,11 @@ static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
     if (p == passes - 1)
       NB_TRY((launch_sort_pass<K, kSortLast>(tiles, st, kin, vin, kalt, valt, a.n, 8 * p,
                                              hist, status, ctr, w.err, a.pos,
-                                             w.pos_sorted, nullptr, 0)));
+                                             w.pos_sorted, nullptr, 0, true)));
     else
       NB_TRY((launch_sort_pass<K, kSortMid>(tiles, st, kin, vin, kalt, valt, a.n, 8 * p,
                                             hist, status, ctr, w.err, nullptr, nullptr,
-                                            nullptr, 0)));
+                                            nullptr, 0, true)));
     K* tk = kin; kin = kalt; kalt = tk;
     uint32_t* tv = vin; vin = valt; valt = tv;
   }
@@ -497,9 +502,9 @@ struct TreeView {
   int n;
   int base;             // first slot of this tree in the arrays of p
   __device__ const float4* ps() const { return p.ps + base; }
-  __device__ Node* nodes() const { return p.nodes + base; }
+  __device__ Node* nodes() const { return p.nodes ? p.nodes + base : nullptr; }
   __device__ PairRec* pairs() const { return p.pairs ? p.pairs + base : nullptr; }
-  __device__ int* parent() const { return p.parent + 2 * (size_t)base; }
+  __device__ int* parent() const { return p.parent ? p.parent + 2 * (size_t)base : nullptr; }
   __device__ double4* sums() const { return p.sums + base; }
   __device__ float4* box_lo() const { return p.box_lo + base; }
   __device__ float4* box_hi() const { return p.box_hi + base; }
@@ -579,14 +584,21 @@ __device__ __forceinline__ void write_node(const TreeView& a, int id, int lo,
   const float e = fmaxf(__fsub_rn(c.hi.x, c.lo.x),
                         fmaxf(__fsub_rn(c.hi.y, c.lo.y), __fsub_rn(c.hi.z, c.lo.z)));
   const float size2 = __fmul_rn(e, e);
-  float4* rec = reinterpret_cast<float4*>(&a.nodes()[id]);
-  rec[0] = com;
-  reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(size2), 0);
-  a.parent()[l] = id;
-  a.parent()[r] = id;
+  if (Node* nd = a.nodes()) {
+    float4* rec = reinterpret_cast<float4*>(&nd[id]);
+    rec[0] = com;
+    reinterpret_cast<int4*>(rec)[1] = make_int4(l, r, __float_as_int(size2), 0);
+  }
+  if (int* par = a.parent()) {
+    par[l] = id;
+    par[r] = id;
+  }
   if (!(lo == 0 && hi == ni)) {
     if (id == hi) write_pair_half(a, id, 0, com, size2, sc);
     else write_pair_half(a, id - 1, 1, com, size2, sc);
+  } else if (PairRec* pr = a.pairs()) {   // the root's own record
+    pr[ni].c[0] = com;
+    reinterpret_cast<float2*>(&pr[ni].sw)[0] = make_float2(size2, __int_as_float(sc));
   }
 }
 
@@ -688,7 +700,7 @@ __device__ __forceinline__ bool finish_node(const TreeView& a, const LevelSmem& 
   const int ni = a.n - 1;
   if (lo == 0 && hi == ni) {   // the root: this run is the whole tree
     write_node(a, 0, lo, hi, sc, c);
-    a.parent()[0] = -1;
+    if (int* par = a.parent()) par[0] = -1;
     return false;
   }
   const bool right = lo == 0 || (hi != ni && sm.delta[ib + 1] > sm.delta[ia]);
@@ -739,9 +751,13 @@ __device__ __forceinline__ void climb_arrival(const TreeView& a, const LevelSmem
   raise_err(a.err(), NB_DEVERR_TREE);
 }
 
+// Later levels hold 2048 items (196 KB of shared memory): one CTA per SM, so
+// they may use twice the registers of the first level's two CTAs.
 template <typename K, bool FIRST>
-__global__ void __launch_bounds__(kLevelThreads, 2) k_build_level(LevelArgs args) {
+__global__ void __launch_bounds__(kLevelThreads, FIRST ? 2 : 1) k_build_level(LevelArgs args) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  chain_release();
+  chain_wait();
   constexpr int C = FIRST ? kLeafGroup : kLevelItems;
   const LevelSmem sm(smem_raw, C);
   // this CTA's tree, its group index there, its input segments [sfirst,
@@ -955,9 +971,9 @@ static LevelArgs level_args(Workspace& w, const StepArgs& a) {
   b.n = a.n;
   b.keys = w.keys;
   b.ps = w.pos_sorted;
-  b.nodes = w.nodes;
+  b.nodes = a.node_records || a.walk_kernel != 0 ? w.nodes : nullptr;
   b.pairs = w.pairs;
-  b.parent = w.parent;
+  b.parent = a.node_records || a.walk_kernel != 0 ? w.parent : nullptr;
   b.sums = w.sums;
   b.box_lo = w.box_lo;
   b.box_hi = w.box_hi;
@@ -983,14 +999,12 @@ int launch_build(Workspace& w, const StepArgs& a, cudaStream_t st) {
   if (a.key_bits == 63) {
     NB_CUDA(cudaFuncSetAttribute(k_build_level<uint64_t, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_build_level<uint64_t, true><<<groups, kLevelThreads, smem, st>>>(b);
+    return launch_chained(k_build_level<uint64_t, true>, groups, kLevelThreads, smem, st, b);
   } else {
     NB_CUDA(cudaFuncSetAttribute(k_build_level<uint32_t, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_build_level<uint32_t, true><<<groups, kLevelThreads, smem, st>>>(b);
+    return launch_chained(k_build_level<uint32_t, true>, groups, kLevelThreads, smem, st, b);
   }
-  NB_CUDA(cudaGetLastError());
-  return NB_OK;
 }
 
 // Later levels: the tree above the leaf groups, up to the root.
@@ -1010,8 +1024,7 @@ int launch_com(Workspace& w, const StepArgs& a, cudaStream_t st) {
     b.in_span = span;
     b.out_seg = next > 1 ? w.seg[p ^ 1] : nullptr;
     b.out_count = next > 1 ? w.seg_count[p ^ 1] : nullptr;
-    k_build_level<uint32_t, false><<<next, kLevelThreads, smem, st>>>(b);
-    NB_CUDA(cudaGetLastError());
+    NB_TRY(launch_chained(k_build_level<uint32_t, false>, next, kLevelThreads, smem, st, b));
     groups = next;
     span *= b.fan;
     p ^= 1;
@@ -1078,8 +1091,10 @@ int launch_ens_morton(const EnsArgs& e, cudaStream_t st) {
 }
 
 // Sorts; on return e.keys / e.perm point at the buffers holding the result.
+int ens_sort_passes() { return (kEnsKeyBits + 7) / 8; }
+
 int launch_ens_sort(EnsArgs& e, cudaStream_t st) {
-  const int passes = (kEnsKeyBits + 7) / 8;
+  const int passes = ens_sort_passes();
   const int tiles = (e.nslots + kSortTile - 1) / kSortTile;
   uint64_t* kin = e.keys;
   uint64_t* kalt = e.keys_alt;
@@ -1161,9 +1176,9 @@ int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st) 
   LevelArgs b{};
   b.keys = e.keys;
   b.ps = e.pos_sorted;
-  b.nodes = e.nodes;
+  b.nodes = nullptr;   // the pair walk reads the child-pair records only
   b.pairs = e.pairs;
-  b.parent = e.parent;
+  b.parent = nullptr;
   b.sums = e.sums;
   b.box_lo = e.box_lo;
   b.box_hi = e.box_hi;

@@ -38,6 +38,7 @@ __device__ __forceinline__ void drift_comp(float& hi, float& lo, float v,
 
 template <bool KD, bool COMP, bool BBOX, bool PACK>
 __global__ void __launch_bounds__(kPrepThreads) k_prep(PrepArgs a) {
+  chain_release();   // the Morton kernel may be scheduled (it waits for this grid)
   int lo[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff};
   int hi[3] = {(int)0x80000000, (int)0x80000000, (int)0x80000000};
   const int stride = gridDim.x * blockDim.x;

@@ -109,6 +109,118 @@ __device__ __forceinline__ float box_far2(float cx, float cy, float cz, float lo
   return fx * fx + fy * fy + fz * fz;
 }
 
+// One tree node as the pair layout holds it: centre of mass (a leaf: its
+// position) and mass in c, size2 (-1 for a leaf, which every opening test
+// accepts) and the split whose record holds its children (-1 for a leaf).
+struct PairNode {
+  float4 c;
+  float size2;
+  int split;
+};
+
+__device__ __forceinline__ PairNode pair_child(const PairRec* __restrict__ pr, int k,
+                                               int side) {
+  PairNode nd;
+  nd.c = pr[k].c[side];
+  const float2 h = reinterpret_cast<const float2*>(&pr[k].sw)[side];
+  nd.size2 = h.x;
+  nd.split = __float_as_int(h.y);
+  return nd;
+}
+
+__device__ __forceinline__ PairNode pair_root(const WalkArgs& a) {
+  const PairRec* r = a.pairs + (a.n - 1);
+  PairNode nd;
+  nd.c = r->c[0];
+  nd.size2 = r->sw.x;
+  nd.split = __float_as_int(r->sw.y);
+  return nd;
+}
+
+// Depth-first walks over the child-pair records, for warps whose stack of
+// opened nodes would overflow: the per-target walk (src/forces_bh.cu:335-377)
+// and the warp-shared one (src/forces_bh.cu:395-447), right child first, with
+// the reference's opening test; a leaf (size2 = -1) always interacts.  Stack
+// entries are 2 * split + side.  `stack` (warp walk): this warp's
+// shared-memory stack of at least kStack entries, written by lane 0 and read
+// after __syncwarp.
+template <bool COUNT>
+__device__ float3 dfs_pair_thread(const WalkArgs& a, float4 bi, int* cnt_out) {
+  const int ni = a.n - 1;
+  float3 ai = make_float3(0.f, 0.f, 0.f);
+  int cnt = 0;
+  int stack[kStack];
+  int sp = 0;
+  PairNode nd = pair_root(a);
+  for (int visits = 0;; ++visits) {   // a valid tree: at most 2n - 1 visits
+    if (visits >= 2 * a.n) {
+      raise_err(a.err, NB_DEVERR_VISITS);
+      break;
+    }
+    const float dx = __fsub_rn(nd.c.x, bi.x), dy = __fsub_rn(nd.c.y, bi.y),
+                dz = __fsub_rn(nd.c.z, bi.z);
+    const float d2 = dist2(dx, dy, dz);
+    if (nd.size2 < __fmul_rn(a.theta2, d2)) {
+      pair_term(ai, dx, dy, dz, d2, nd.c.w, a.eps2);
+      if (COUNT) ++cnt;
+    } else {
+      if (sp >= kStack || (unsigned)nd.split >= (unsigned)ni) {
+        raise_err(a.err, sp >= kStack ? NB_DEVERR_STACK : NB_DEVERR_TREE);
+        break;
+      }
+      stack[sp++] = 2 * nd.split;
+      nd = pair_child(a.pairs, nd.split, 1);
+      continue;
+    }
+    if (sp == 0) break;
+    const int e = stack[--sp];
+    nd = pair_child(a.pairs, e >> 1, e & 1);
+  }
+  if (COUNT) *cnt_out = cnt;
+  return ai;
+}
+
+template <bool COUNT>
+__device__ float3 dfs_pair_warp(const WalkArgs& a, float4 bi, bool live, int* stack,
+                                int* cnt_out) {
+  const int lane = threadIdx.x & 31;
+  const int ni = a.n - 1;
+  float3 ai = make_float3(0.f, 0.f, 0.f);
+  int cnt = 0;
+  int sp = 0;
+  PairNode nd = pair_root(a);
+  for (int visits = 0;; ++visits) {
+    if (visits >= 2 * a.n) {
+      if (lane == 0) raise_err(a.err, NB_DEVERR_VISITS);
+      break;
+    }
+    const float dx = __fsub_rn(nd.c.x, bi.x), dy = __fsub_rn(nd.c.y, bi.y),
+                dz = __fsub_rn(nd.c.z, bi.z);
+    const float d2 = dist2(dx, dy, dz);
+    const bool open = live && !(nd.size2 < __fmul_rn(a.theta2, d2));
+    if (__any_sync(0xffffffffu, open)) {   // uniform: nd is the same in every lane
+      if (sp >= kStack || (unsigned)nd.split >= (unsigned)ni) {
+        if (lane == 0) raise_err(a.err, sp >= kStack ? NB_DEVERR_STACK : NB_DEVERR_TREE);
+        break;
+      }
+      if (lane == 0) stack[sp] = 2 * nd.split;
+      ++sp;
+      __syncwarp();
+      nd = pair_child(a.pairs, nd.split, 1);
+      continue;
+    }
+    pair_term(ai, dx, dy, dz, d2, nd.c.w, a.eps2);
+    if (COUNT) ++cnt;
+    if (sp == 0) break;
+    --sp;
+    const int e = stack[sp];
+    __syncwarp();   // all lanes have read the slot before it is reused
+    nd = pair_child(a.pairs, e >> 1, e & 1);
+  }
+  if (COUNT) *cnt_out = cnt;
+  return ai;
+}
+
 // The walk of warp `wg` (targets 32wg .. 32wg+31); all 32 lanes call it.
 template <int W, bool MASKED, bool COUNT, bool HOIST = false>
 __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
@@ -199,15 +311,15 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
   // the root: one exact test per target (dead lanes repeat a live one)
   int sp = 0;
   {
-    const Node root = a.nodes[0];
-    const bool acc = accepts(root.size2, theta2, root.com.x, root.com.y, root.com.z,
+    const PairNode root = pair_root(a);
+    const bool acc = accepts(root.size2, theta2, root.c.x, root.c.y, root.c.z,
                              bi.x, bi.y, bi.z);
-    const int sc0 = root.left < ni ? root.left : root.left - ni;
+    const int sc0 = min(max(root.split, 0), ni - 1);   // a valid tree never needs the clamp
     const unsigned am = MASKED ? (__ballot_sync(full, acc) & live_mask)
                                : (__all_sync(full, acc) ? live_mask : 0u);
     if (lane == 0) {
       if (am) {
-        put_entry(ent, 0, root.com.x, root.com.y, root.com.z, root.com.w);
+        put_entry(ent, 0, root.c.x, root.c.y, root.c.z, root.c.w);
         if (MASKED) sm.emask[w][0] = am;
       }
       if (am != live_mask) {
@@ -406,9 +518,9 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     cnt = 0;
     __syncwarp();
     if (MASKED)
-      ai = dfs_walk_thread<COUNT>(a, bi, &cnt);
+      ai = dfs_pair_thread<COUNT>(a, bi, &cnt);
     else
-      ai = dfs_walk_warp<COUNT>(a, bi, live, sm.stk[w], &cnt);
+      ai = dfs_pair_warp<COUNT>(a, bi, live, sm.stk[w], &cnt);
   }
   if (live) {
     epilogue(a, t, ai);
@@ -421,6 +533,7 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
 template <int W, bool MASKED, bool COUNT>
 __global__ void __launch_bounds__(W * 32, 32 / W) k_walk_pair(WalkArgs a) {
   __shared__ PairSmem<W, MASKED> sm;
+  chain_wait();
   walk_pair_warp<W, MASKED, COUNT>(a, a.t0 / 32 + blockIdx.x * W + (threadIdx.x >> 5), sm);
 }
 
@@ -457,7 +570,7 @@ __global__ void __launch_bounds__(kEnsW * 32) k_walk_pair_ens(EnsArgs e) {
     a.n = d.n;
     a.ps = e.pos_sorted + d.base;
     a.perm = e.perm + d.base;
-    a.nodes = e.nodes + d.base;
+    a.nodes = nullptr;   // the pair layout is the whole tree here
     a.pairs = e.pairs + d.base;
     a.theta2 = d.theta2;
     a.eps2 = d.eps2;
@@ -510,18 +623,17 @@ int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
 }
 
 template <int W>
-static void launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaStream_t st) {
+static int launch_walk_pair_w(const WalkArgs& a, bool masked, int blocks, cudaStream_t st) {
   if (masked) {
     // the lane masks double the stack: thread semantics stay at <= 4 warps
     // per block (<= 32 KB of static shared memory)
     constexpr int WM = W < 4 ? W : 4;
     const int bm = (blocks * W + WM - 1) / WM;
-    if (a.counts) k_walk_pair<WM, true, true><<<bm, WM * 32, 0, st>>>(a);
-    else k_walk_pair<WM, true, false><<<bm, WM * 32, 0, st>>>(a);
-  } else {
-    if (a.counts) k_walk_pair<W, false, true><<<blocks, W * 32, 0, st>>>(a);
-    else k_walk_pair<W, false, false><<<blocks, W * 32, 0, st>>>(a);
+    return a.counts ? launch_chained(k_walk_pair<WM, true, true>, bm, WM * 32, 0, st, a)
+                    : launch_chained(k_walk_pair<WM, true, false>, bm, WM * 32, 0, st, a);
   }
+  return a.counts ? launch_chained(k_walk_pair<W, false, true>, blocks, W * 32, 0, st, a)
+                  : launch_chained(k_walk_pair<W, false, false>, blocks, W * 32, 0, st, a);
 }
 
 // The block shape (warps per block) is the tuning table's.
@@ -530,11 +642,9 @@ int launch_walk_pair(const WalkArgs& a, bool masked, cudaStream_t st) {
   if (warps <= 0) return NB_OK;
   const int W = tune_walk_warps();
   const int blocks = (warps + W - 1) / W;
-  if (W == 2) launch_walk_pair_w<2>(a, masked, blocks, st);
-  else if (W == 8) launch_walk_pair_w<8>(a, masked, blocks, st);
-  else launch_walk_pair_w<4>(a, masked, blocks, st);
-  NB_CUDA(cudaGetLastError());
-  return NB_OK;
+  if (W == 2) return launch_walk_pair_w<2>(a, masked, blocks, st);
+  if (W == 8) return launch_walk_pair_w<8>(a, masked, blocks, st);
+  return launch_walk_pair_w<4>(a, masked, blocks, st);
 }
 
 int warm_walk_pair_kernels() {

@@ -53,7 +53,10 @@ struct __align__(16) Node {
 // which every opening test accepts) and w the split of an internal child,
 // where its own children are recorded (-1 for a leaf).  The tree build writes
 // each child's half (one 16-byte and one 8-byte store) when it finishes the
-// child; the root is the one node with no record.
+// child.  The root, the one node that is nobody's child, has its own record
+// at k = n - 1: c[0] its centre of mass and mass, sw.x its size2, sw.y its
+// split.  The Barnes-Hut walks of the pair layout need nothing else from the
+// tree; the Node records are written only for the walks that read them.
 struct __align__(16) PairRec {
   float4 c[2];
   float4 sw;
@@ -96,7 +99,7 @@ struct Workspace {
   uint32_t* vals_alt = nullptr;
   float4* pos_sorted = nullptr;   // [cap]
   Node* nodes = nullptr;          // [cap-1]
-  PairRec* pairs = nullptr;       // [cap-1] child pairs by split
+  PairRec* pairs = nullptr;       // [cap] child pairs by split + the root's
   int* parent = nullptr;          // [2cap-1]
   int2* seg[2] = {nullptr, nullptr};      // open splits per build CTA,
   int* seg_count[2] = {nullptr, nullptr}; // ping-pong between levels
@@ -157,6 +160,9 @@ struct StepArgs {
   int key_bits;
   int traverse;
   int walk_kernel;  // 0 pair walk, 1 depth-first walk, 2 list walk
+  // the tree build also writes the Node records and parent links (walk
+  // kernels 1 and 2 read them, nb_debug_lbvh returns them)
+  bool node_records = false;
   bool kick_drift;  // opening kick + drift before the force evaluation
   bool kick_after;  // closing kick fused into the force epilogue
   int* counts;      // debug: interactions per sorted target, or nullptr
@@ -217,6 +223,47 @@ inline int warm_fns(F* kernel, R*... rest) {
   NB_TRY(warm_fn(kernel));
   return warm_fns(rest...);
 }
+// Programmatic dependent launch along the one-simulation Barnes-Hut chain
+// (Morton keys, sort passes, build levels, walk).  A kernel launched with
+// launch_chained may be scheduled while the kernel before it in the stream
+// is still running: it calls chain_wait() before its first memory access
+// (griddepcontrol.wait returns once the predecessor grid has completed and
+// its writes are visible; in a kernel launched without the attribute it
+// returns at once), and each kernel of the chain calls chain_release() at
+// its start, which lets its successor's CTAs be scheduled once all of its
+// own CTAs are running.  What overlaps is launch and CTA set-up, never data.
+// Only eager launches carry the attribute: measured on a B200, the chain
+// gains 2-4 % launched kernel by kernel, and a captured step graph with
+// programmatic edges ran slower than the plain graph (13 % at N = 100,000,
+// equal at 1M), so launches under stream capture stay plain.
+__device__ __forceinline__ void chain_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void chain_release() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+inline int launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                          cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    cs = cudaStreamCaptureStatusNone;
+  }
+  cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
+  NB_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+  return NB_OK;
+}
+
 int warm_kernels();
 int warm_prep_kernels();
 int warm_lbvh_kernels();
@@ -311,6 +358,7 @@ struct SimDesc {
 constexpr int kEnsSimBits = 10;                     // sim id field of the keys
 constexpr int kEnsMaxSims = (1 << kEnsSimBits) - 1; // id 1023 marks unused slots
 constexpr int kEnsKeyBits = 30 + kEnsSimBits;       // 40 bits, 5 sort passes
+int ens_sort_passes();
 
 // One CTA of a multi-tree build level.
 struct BuildRun {
@@ -346,9 +394,7 @@ struct EnsArgs {
   uint64_t* keys_alt;
   uint32_t* perm;             // [nslots] x2: original slot of each sorted slot
   uint32_t* perm_alt;
-  Node* nodes;                // [nslots]
-  PairRec* pairs;             // [nslots] child pairs by split
-  int* parent;                // [2 nslots]
+  PairRec* pairs;             // [nslots] child pairs by split + each root's
   double4* sums;              // [nslots]
   float4* box_lo;
   float4* box_hi;

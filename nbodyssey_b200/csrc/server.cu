@@ -35,9 +35,8 @@ using namespace nb;
 
 namespace {
 
-constexpr size_t kBytesPerSlot = 272;   // state 64, sorted 16, keys 16, perm 8,
-                                        // nodes 32, child pairs 48, parent 8,
-                                        // sums 32, boxes 32,
+constexpr size_t kBytesPerSlot = 232;   // state 64, sorted 16, keys 16, perm 8,
+                                        // child pairs 48, sums 32, boxes 32,
                                         // sort scratch ~12, build plan and
                                         // segments ~4
 constexpr int kInFlight = 2;            // engine steps queued ahead of the GPU
@@ -523,9 +522,7 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
     if ((rc = srv_alloc(s, &e.keys_alt, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.perm, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.perm_alt, S)) != NB_OK) break;
-    if ((rc = srv_alloc(s, &e.nodes, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.pairs, S)) != NB_OK) break;
-    if ((rc = srv_alloc(s, &e.parent, 2 * S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.sums, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.box_lo, S)) != NB_OK) break;
     if ((rc = srv_alloc(s, &e.box_hi, S)) != NB_OK) break;
@@ -565,10 +562,8 @@ int nb_server_create(size_t hbm_budget_bytes, int max_sims, nb_server** out) {
       ce = cudaEventCreateWithFlags(&s->frame_staged[k], cudaEventDisableTiming);
       if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&s->frame_copied[k], cudaEventDisableTiming);
     }
-    if (ce == cudaSuccess) ce = cudaMemset(e.parent, 0xff, 2 * S * sizeof(int));
     if (ce == cudaSuccess) ce = cudaMemset(e.perm, 0, S * 4);
     if (ce == cudaSuccess) ce = cudaMemset(e.perm_alt, 0, S * 4);
-    if (ce == cudaSuccess) ce = cudaMemset(e.nodes, 0, S * sizeof(Node));
     if (ce == cudaSuccess) ce = cudaMemset(e.pairs, 0, S * sizeof(PairRec));
     if (ce == cudaSuccess) ce = cudaMemset(e.hist, 0, words * 4);
     if (ce == cudaSuccess) ce = cudaMemset(e.err, 0, 16);

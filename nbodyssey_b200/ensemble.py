@@ -96,6 +96,12 @@ class Ensemble:
         L.check(self._lib.nb_ensemble_force(self._h, int(sim), ctypes.byref(f)))
         return "naive" if f.value == L.NB_FORCE_NAIVE else "bh"
 
+    def kernels_per_step(self):
+        """Kernel launches of one step of this ensemble."""
+        k = ctypes.c_int()
+        L.check(self._lib.nb_ensemble_kernels_per_step(self._h, ctypes.byref(k)))
+        return k.value
+
     def record(self, slot):
         L.check(self._lib.nb_ensemble_record(self._h, int(slot)))
 

@@ -97,6 +97,20 @@ def test_large_tree_bit_exact_1m():
     assert abs(float(t["com4"][0, 3]) - float(pos[:, 3].astype(np.float64).sum())) < 1e-5
 
 
+@pytest.mark.parametrize("n,bits,layout", [(4_194_305, 30, "disks"), (300_001, 63, "disks"),
+                                           (300_001, 30, "coincident")])
+def test_levels_above_groups_bit_exact(n, bits, layout):
+    """Trees with several levels above the 1024-leaf groups (4M: four
+    later launches; coincident points: the longest open-split segments)."""
+    if layout == "coincident":
+        pos = np.zeros((n, 4), np.float32)
+        pos[:, :3] = -0.75
+        pos[:, 3] = 1.0 / n
+    else:
+        pos, _ = ic.two_disks(n, seed=n)
+    _assert_tree_equal(_device_tree(pos, bits), O.Tree(pos, bits), bits)
+
+
 def expected_pairs(o):
     """The child-pair records implied by the oracle's tree: record k holds the
     children of the internal node whose split is after sorted leaf k."""
