@@ -47,10 +47,11 @@ METRIC = ("steps/s at 1M (BH θ=0.5); served particle-steps/s + p99 vs "
 N_DEFAULT = 1_000_000
 FLOP_PER_PAIR = 20          # src/main.cu:203-207 convention
 # algorithmic HBM bytes per particle of the step before the walk: kick, drift
-# and box 112 (r pos, lo, vel, acc; w pos, lo, vel), Morton keys 24, four
-# sort passes 64, sorted-position gather 32, first build level 68 (r keys,
-# sorted positions; w two 24-byte child-pair halves per particle)
-BUILD_BYTES_PER_PARTICLE = 300
+# and box 112 (r pos, lo, vel, acc; w pos, lo, vel), Morton keys 20 (r pos,
+# w key), four sort passes 60 (the first reads no values), sorted-position
+# gather 32, first build level 68 (r keys, sorted positions; w two 24-byte
+# child-pair halves per particle)
+BUILD_BYTES_PER_PARTICLE = 292
 HBM_FALLBACK_GBS = 6650.0   # copy bandwidth measured on this pool's B200s (no peaks file)
 L2_FLUSH_BYTES = 256 << 20
 
@@ -487,8 +488,8 @@ def run_b200(args, rank, world, local, pg):
                            "peak": hbm, "unit": "GB/s",
                            "frac": (BUILD_BYTES_PER_PARTICLE * n / (build_ms * 1e-3) / 1e9
                                     / hbm),
-                           "work": "300 B/particle (kick, drift and box 112, keys 24, "
-                                   "4 sort passes 64, gather 32, child-pair records 68)",
+                           "work": "292 B/particle (kick, drift and box 112, keys 20, "
+                                   "4 sort passes 60, gather 32, child-pair records 68)",
                            "peak_source": hbm_src},
         "clocks": clk,
     }

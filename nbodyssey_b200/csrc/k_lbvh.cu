@@ -45,8 +45,7 @@ constexpr int kMortonThreads = 1024;
 template <typename K>
 __global__ void __launch_bounds__(kMortonThreads) k_morton(const float4* __restrict__ pos,
                                                 int n, const int* __restrict__ bbox,
-                                                K* keys, uint32_t* vals,
-                                                uint32_t* hist, int passes) {
+                                                K* keys, uint32_t* hist, int passes) {
   chain_release();
   chain_wait();
   __shared__ uint32_t s_hist[8 * kSortRadix];
@@ -83,7 +82,6 @@ __global__ void __launch_bounds__(kMortonThreads) k_morton(const float4* __restr
       else
         k = (K)((spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz));
       keys[i] = k;
-      vals[i] = (uint32_t)i;
       for (int ps = 0; ps < passes; ++ps)
         atomicAdd(&s_hist[ps * kSortRadix + (uint32_t)((k >> (8 * ps)) & 0xffu)], 1u);
     }
@@ -103,10 +101,10 @@ int launch_morton(Workspace& w, const StepArgs& a, cudaStream_t st) {
   if (a.key_bits == 63)
     return launch_chained(k_morton<uint64_t>, blocks, kMortonThreads, 0, st,
                           (const float4*)a.pos, a.n, (const int*)w.bbox,
-                          (uint64_t*)w.keys, w.vals, w.hist, passes);
+                          (uint64_t*)w.keys, w.hist, passes);
   return launch_chained(k_morton<uint32_t>, blocks, kMortonThreads, 0, st,
                         (const float4*)a.pos, a.n, (const int*)w.bbox, (uint32_t*)w.keys,
-                        w.vals, w.hist, passes);
+                        w.hist, passes);
 }
 
 // ---------------------------------------------------------------------------
@@ -206,7 +204,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortCtasPerSm)
     long idx = seg + k * 32 + lane;
     bool ok = idx < n;
     key[k] = ok ? kin[idx] : (K)0;
-    val[k] = ok ? vin[idx] : 0u;
+    val[k] = ok ? (vin ? vin[idx] : (uint32_t)idx) : 0u;   // no vin: the identity
   }
   const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
@@ -389,8 +387,11 @@ static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
   const int tiles = (a.n + kSortTile - 1) / kSortTile;
   K* kin = (K*)w.keys;
   K* kalt = (K*)w.keys_alt;
-  uint32_t* vin = w.vals;
+  // the first pass takes the particle index as its value (the keys are in
+  // particle order), so no value array is read before it
+  uint32_t* vin = nullptr;
   uint32_t* valt = w.vals_alt;
+  uint32_t* vnext = w.vals;   // the second pass's output
   for (int p = 0; p < passes; ++p) {
     uint32_t* hist = w.hist + p * kSortRadix;
     uint32_t* status = w.hist + 8 * kSortRadix + 8 + (size_t)p * w.status_tiles * kSortRadix;
@@ -404,7 +405,7 @@ static int sort_impl(Workspace& w, const StepArgs& a, cudaStream_t st) {
                                             hist, status, ctr, w.err, nullptr, nullptr,
                                             nullptr, 0, true)));
     K* tk = kin; kin = kalt; kalt = tk;
-    uint32_t* tv = vin; vin = valt; valt = tv;
+    uint32_t* tv = valt; valt = vnext; vin = tv; vnext = tv;
   }
   // after an even number of passes the result is back in keys / vals
   if (kin != (K*)w.keys) {
