@@ -275,12 +275,15 @@ __device__ __forceinline__ void walk_pair_warp(const WalkArgs& a, int wg,
     const ulonglong2 B = *reinterpret_cast<const ulonglong2*>(&base[q * 8 + 4]);
     f2 m = B.y;
     if (MASKED) {
-      const unsigned b0 = (sm.emask[w][at + 2 * q] >> lane) & 1u;
-      const unsigned b1 = (sm.emask[w][at + 2 * q + 1] >> lane) & 1u;
+      // the pair's two lane masks in one load (at + 2q is even, the row
+      // 16-byte aligned); this lane's bit keeps or zeroes each mass
+      const uint2 mk = *reinterpret_cast<const uint2*>(&sm.emask[w][at + 2 * q]);
+      const unsigned lbit = lt + 1u;
+      const bool b0 = (mk.x & lbit) != 0u, b1 = (mk.y & lbit) != 0u;
       float m0, m1;
       up2(B.y, m0, m1);
       m = pk2(b0 ? m0 : 0.f, b1 ? m1 : 0.f);
-      if (COUNT) cnt += (int)(b0 + b1);
+      if (COUNT) cnt += (int)b0 + (int)b1;
     }
     f2 dx = add2(A.x, qx);
     f2 dy = add2(A.y, qy);
