@@ -381,6 +381,8 @@ struct nb_sim {
   // nb_step_host: positions leave on a side stream once the drift is done
   cudaStream_t io_stream = nullptr;
   cudaEvent_t io_prep = nullptr;
+  cudaEvent_t io_in = nullptr;    // host-state steps: positions uploaded
+  cudaEvent_t io_vel = nullptr;   // host-state steps: velocities uploaded
   // nb_step_host_state: uploaded positions, and whether they differ from the
   // simulation's own
   float4* pos_in = nullptr;
@@ -405,6 +407,8 @@ static void sim_free(nb_sim* s) {
     cudaStreamDestroy(s->io_stream);
   }
   if (s->io_prep) cudaEventDestroy(s->io_prep);
+  if (s->io_in) cudaEventDestroy(s->io_in);
+  if (s->io_vel) cudaEventDestroy(s->io_vel);
   cudaFree(s->pos_in);
   cudaFree(s->d_diff);
   if (s->h_diff) cudaFreeHost(s->h_diff);
@@ -768,13 +772,20 @@ int nb_step_host_state(nb_sim* s, const float* pos4, const float* vel4, float* p
   if (!s->io_stream)
     NB_CUDA(cudaStreamCreateWithFlags(&s->io_stream, cudaStreamNonBlocking));
   if (!s->io_prep) NB_CUDA(cudaEventCreateWithFlags(&s->io_prep, cudaEventDisableTiming));
+  if (!s->io_in) NB_CUDA(cudaEventCreateWithFlags(&s->io_in, cudaEventDisableTiming));
+  if (!s->io_vel) NB_CUDA(cudaEventCreateWithFlags(&s->io_vel, cudaEventDisableTiming));
   if (!s->pos_in) NB_TRY(dalloc(&s->pos_in, s->n));
   if (!s->d_diff) NB_TRY(dalloc(&s->d_diff, 1));
   if (!s->h_diff) NB_CUDA(cudaMallocHost((void**)&s->h_diff, sizeof(unsigned)));
   const size_t b = sizeof(float4) * s->n;
   cudaStream_t st = s->stream;
-  NB_CUDA(cudaMemcpyAsync(s->vel, vel4, b, cudaMemcpyHostToDevice, st));
+  // positions first; the velocities follow on the side stream while the
+  // positions are compared with the simulation's own
   NB_CUDA(cudaMemcpyAsync(s->pos_in, pos4, b, cudaMemcpyHostToDevice, st));
+  NB_CUDA(cudaEventRecord(s->io_in, st));
+  NB_CUDA(cudaStreamWaitEvent(s->io_stream, s->io_in, 0));
+  NB_CUDA(cudaMemcpyAsync(s->vel, vel4, b, cudaMemcpyHostToDevice, s->io_stream));
+  NB_CUDA(cudaEventRecord(s->io_vel, s->io_stream));
   // a(x) and the low-order position parts on the device belong to the
   // simulation's positions: they carry on when the caller hands those back
   bool same = false;
@@ -790,6 +801,7 @@ int nb_step_host_state(nb_sim* s, const float* pos4, const float* vel4, float* p
     NB_CUDA(cudaMemsetAsync(s->pos_lo, 0, b, st));
     NB_TRY(sim_forces(s, nullptr));
   }
+  NB_CUDA(cudaStreamWaitEvent(st, s->io_vel, 0));   // the kick reads the velocities
   StepArgs a = sim_args(s);
   a.kick_drift = true;
   a.kick_after = true;
