@@ -76,3 +76,22 @@ def test_ensemble_rejects_unsupported_params():
     assert ei.value.code == L.NB_ERR_INVALID
     with pytest.raises(L.NbError):
         Ensemble([(pos, vel)], api.SimParams(force="bh", epsilon=0.0))
+
+
+def test_ensemble_kernels_per_step():
+    """The launch count a step reports: prep, then the tree pipeline (Morton
+    keys, five sort passes, the build levels, one walk launch per semantics
+    in use) when some simulation uses Barnes-Hut, and the all-pairs packing
+    plus one queue launch per launch shape when some uses all-pairs."""
+    states, params = _mix(("bh",))
+    warp_only = [dataclasses.replace(p, traverse="warp") for p in params]
+    with Ensemble(states, warp_only) as ens:
+        k_warp = ens.kernels_per_step()
+    with Ensemble(states, params) as ens:
+        k_both = ens.kernels_per_step()
+    assert k_both == k_warp + 1                 # a second walk launch
+    assert k_warp >= 1 + 1 + 5 + 1 + 1          # prep, Morton, sort, >= 1 level, walk
+    states, params = _mix(("naive",))
+    with Ensemble(states, params) as ens:
+        k_ap = ens.kernels_per_step()
+    assert 3 <= k_ap <= 1 + 1 + 6               # prep, pack, 1..6 queue shapes
