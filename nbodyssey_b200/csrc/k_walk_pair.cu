@@ -33,7 +33,7 @@
 // (x0,x1,y0,y1)(z0,z1,m0,m1)), evaluated 32 at a time by an unrolled body
 // with packed FP32 math, two entries per instruction; entries whose mask
 // excludes a lane contribute with mass 0.  A stack that would overflow hands
-// the warp to the depth-first walk of the same semantics.
+// the warp to a depth-first walk of the same semantics over the same records.
 #include <algorithm>
 #include <cmath>
 #include <vector>

@@ -1,4 +1,4 @@
-// Pieces shared by the tree walks (k_walk.cu, k_walk_list.cu).
+// Pieces shared by the tree walks (k_walk.cu, k_walk_list.cu, k_walk_pair.cu).
 //
 // Opening test, in this exact float order (the CPU oracle repeats it, so the
 // interaction sets match bit for bit; src/forces_bh.cu:352-356):
@@ -15,7 +15,7 @@ struct WalkArgs {
   int n;
   const float4* __restrict__ ps;      // sorted positions
   const uint32_t* __restrict__ perm;  // sorted -> original
-  const Node* __restrict__ nodes;
+  const Node* __restrict__ nodes;     // Node records (walk kernels 1 and 2)
   const PairRec* __restrict__ pairs;  // child pairs by split (pair walk)
   float theta2, eps2, G, half_dt;
   float4* acc;       // original order
