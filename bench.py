@@ -314,11 +314,17 @@ def measured_peaks():
         return {}
 
 
-def profiled_traffic(kernel):
+def profiled_traffic(kernel, traverse="warp", theta=0.5):
     """Per-launch DRAM bytes of the timed force kernel from its committed ncu
-    summary (profiles/<kernel>_1m.md, the same 1M workload), if present."""
-    name = {"k_walk_pair": "walk_pair_1m.md", "k_walk_list": "walk_list_1m.md",
-            "k_walk_warp": "walk_warp_dfs_1m.md"}.get(kernel)
+    summary (profiles/<kernel>_1m.md, the same 1M workload at theta 0.5), if
+    present."""
+    if theta != 0.5:
+        return None
+    name = {("k_walk_pair", "warp"): "walk_pair_1m.md",
+            ("k_walk_pair", "thread"): "walk_pair_thread_1m.md",
+            ("k_walk_list", "warp"): "walk_list_1m.md",
+            ("k_walk_list", "thread"): "walk_list_thread_1m.md",
+            ("k_walk_warp", "warp"): "walk_warp_dfs_1m.md"}.get((kernel, traverse))
     if name is None:
         return None
     path = os.path.join(ROOT, "profiles", name)
@@ -449,7 +455,8 @@ def run_b200(args, rank, world, local, pg):
         hbm, hbm_src = HBM_FALLBACK_GBS, "6,650 GB/s copy bandwidth (of fallback)"
     kernel = ({"pair": "k_walk_pair", "list": "k_walk_list"}.get(
         args.walk, "k_walk_%s" % args.traverse) if args.force == "bh" else "k_allpairs")
-    traffic = profiled_traffic(kernel) if args.n == N_DEFAULT else None
+    traffic = (profiled_traffic(kernel, args.traverse, args.theta)
+               if args.n == N_DEFAULT and args.force == "bh" else None)
     line = {
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
