@@ -93,7 +93,7 @@ int ens_enqueue(nb_ensemble* h, bool prime) {
     NB_TRY(launch_ens_morton(e, st));
     NB_TRY(launch_ens_sort(e, st));
     NB_TRY(launch_ens_levels(e, h->plan, st));
-    NB_TRY(launch_walk_list_ens(e, st));
+    NB_TRY(launch_walk_pair_ens(e, st));
   }
   NB_TRY(launch_ens_allpairs(e, h->ap, st));
   return NB_OK;

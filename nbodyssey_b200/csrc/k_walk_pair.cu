@@ -611,7 +611,7 @@ void plan_walk_queue(const SimDesc* sims, int nsims, std::vector<int> items[2]) 
   }
 }
 
-int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st) {
+int launch_walk_pair_ens(const EnsArgs& e, cudaStream_t st) {
   NB_CUDA(cudaMemsetAsync(e.walk_ctr, 0, 2 * sizeof(int), st));
   const int cap = device_sm_count() * 8;   // 8 resident blocks of 4 warps per SM
   for (int q = 0; q < 2; ++q) {

@@ -469,7 +469,7 @@ int launch_ens_sort(EnsArgs& e, cudaStream_t st);   // updates e.keys / e.perm
 int plan_build(const SimDesc* sims, int nsims, BuildPlan& plan);
 size_t plan_seg_entries(int slots, int nsims);
 int launch_ens_levels(const EnsArgs& e, const BuildPlan& plan, cudaStream_t st);
-int launch_walk_list_ens(const EnsArgs& e, cudaStream_t st);
+int launch_walk_pair_ens(const EnsArgs& e, cudaStream_t st);
 // Host: the walk queue of a simulation table (the Barnes-Hut simulations'
 // 32-slot blocks per semantics, costliest simulation first: larger n and
 // smaller theta walk longer); items[0] / items[1] get the warp / thread

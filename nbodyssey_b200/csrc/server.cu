@@ -398,7 +398,7 @@ int engine_iteration(nb_server* s, std::unique_lock<std::mutex>& lk) {
     NB_TRY(launch_ens_morton(e, s->stream));
     NB_TRY(launch_ens_sort(e, s->stream));
     NB_TRY(launch_ens_levels(e, s->plan, s->stream));
-    NB_TRY(launch_walk_list_ens(e, s->stream));
+    NB_TRY(launch_walk_pair_ens(e, s->stream));
   }
   NB_TRY(launch_ens_allpairs(e, s->ap, s->stream));
   NB_CUDA(cudaEventRecord(ev, s->stream));
